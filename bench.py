@@ -1,0 +1,484 @@
+"""Benchmark of the RK3 time-step loop on one or more B200s.
+
+Workload (one "step" = one Shu-Osher RK3 step = 3 RHS evaluations + stage
+updates + the CFL reduction): decaying isotropic turbulence at 256^3, turbulent
+Mach 0.5, Re 1000, Ma 0.5, Pr 0.72, gamma 1.4, Steger-Warming + WENO5, C8th
+viscous terms, CFL 0.5, seeded random-phase solenoidal field with
+E(k) ~ k^4 exp(-2 (k/4)^2) (synthetic; the reference publishes no dataset).
+
+Headline `value`: RK3 steps/s of the FP32-stencil / FP64-accumulation form,
+device-timed with CUDA events on the library's stream (max over ranks).
+Also reported: the plain FP64 form's steps/s, Gcell/s, errors of the FP32 form
+against the FP64 form after a fixed-dt run, the per-kernel roofline, clocks,
+an end-to-end number through the public API with host buffers, and the
+reference CPU path timed on this host's cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: launched under torchrun; every rank runs an independent replica
+(the path does not shard: replicas only), scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 256
+WORKLOAD = dict(gamma=1.4, Pr=0.72, Ma=0.5, Re=1000.0, cfl=0.5, mach_t=0.5, k0=4.0, seed=12345,
+                fvs="stagerwarming", recon="weno5", vis="c8th")
+METRIC = "RK3 steps/s & Gcell/s at 256^3 FP32 vs FP64 at stated err; adjoint/fwd cost"
+STEP_BYTES_PER_CELL = 360.0   # 3 stages x (read U 40 + read U0 40 + write U 40)
+CPU_SAMPLE_N = 64
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------
+# multi-rank plumbing
+# ----------------------------------------------------------------------------
+
+def dist_init(world: int, use_cuda: bool):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl" if use_cuda else "gloo",
+                            timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def dist_max(dist, value: float, use_cuda: bool) -> float:
+    """Max of a float over ranks (every rank calls it)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if use_cuda else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(dist, use_cuda: bool):
+    if dist is None:
+        return
+    import torch
+    if use_cuda:
+        t = torch.zeros(1, device="cuda")
+        dist.all_reduce(t)
+        torch.cuda.synchronize()
+    else:
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(name)
+        out.update(sm_mhz=statistics.median(sm) if sm else None,
+                   sm_max_mhz=max(mx) if mx else None, reasons=sorted(reasons),
+                   samples=len(rows))
+        return out
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+
+def make_params(ns, n, precision, dt_fixed=-1.0):
+    w = WORKLOAD
+    two_pi = 2 * math.pi
+    return ns.SolverParams.default().replace(
+        n=n, gamma=w["gamma"], Pr=w["Pr"], Ma=w["Ma"], Re=w["Re"], cfl=w["cfl"],
+        dt_fixed=dt_fixed, fvs_type=w["fvs"], recon=w["recon"], vis_scheme=w["vis"],
+        Lx=two_pi, Ly=two_pi, Lz=two_pi, precision=precision)
+
+
+def workload_input(n):
+    from ns3d_cpp_b200 import initial
+    w = WORKLOAD
+    return initial.isotropic(n, mach_t=w["mach_t"], Ma=w["Ma"], gamma=w["gamma"], k0=w["k0"],
+                             seed=w["seed"])
+
+
+def kernel_bytes_per_cell(cls: str, rsize: int) -> float:
+    """Algorithmic (compulsory) HBM bytes per cell of one launch of a kernel class."""
+    w = 5 * 8          # rho,u,v,w,p read once
+    if cls == "sweep_x":
+        return w + 5 * rsize
+    if cls in ("sweep_y", "sweep_z"):
+        return w + 10 * rsize
+    if cls == "visc_flux":
+        return 4 * 8 + 9 * rsize
+    if cls == "update":
+        return 2 * w + 5 * rsize + 9 * rsize + 6 * 8
+    return 0.0
+
+
+def timed_steps(torch, s, steps: int, warmup: int, dist, use_cuda, profile=True):
+    """W untimed steps, then K steps bracketed by barrier + synchronize, timed
+    with CUDA events recorded on the library's own stream."""
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    for _ in range(warmup):
+        s.step(1)
+    s.synchronize()
+    dist_barrier(dist, use_cuda)
+    torch.cuda.synchronize()
+    if profile:
+        s.profile(True)
+    l0 = s.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = s.launch_count() - l0
+    prof = s.profile_read() if profile else {}
+    if profile:
+        s.profile(False)
+    dist_barrier(dist, use_cuda)
+    return ms, launches, prof
+
+
+def error_run(ns, n, W, steps, device):
+    """FP32-stencil vs FP64 after `steps` steps at the same fixed dt."""
+    with ns.Solver(make_params(ns, n, "fp64"), device=device) as s:
+        s.upload_primitive(W)
+        dt0 = s.compute_timestep()
+    res = {}
+    for prec in ("fp64", "fp32acc64"):
+        with ns.Solver(make_params(ns, n, prec, dt_fixed=dt0), device=device) as s:
+            s.upload_primitive(W)
+            s.step(steps)
+            st = s.compute_turbulence_statistics()
+            Ek = s.compute_energy_spectrum()
+            res[prec] = (st, Ek)
+    (a, Ea), (b, Eb) = res["fp64"], res["fp32acc64"]
+    big = Ea > 1e-6 * Ea.max()
+
+    def rel(x, y):
+        return abs(x - y) / abs(y)
+    return {"steps": steps, "dt": dt0,
+            "total_energy": rel(b["total_energy"], a["total_energy"]),
+            "kinetic_energy": rel(b["kinetic_energy"], a["kinetic_energy"]),
+            "dissipation": rel(b["dissipation"], a["dissipation"]),
+            "spectrum_max": float(np.max(np.abs(Eb[big] - Ea[big]) / Ea[big])),
+            "reference": "FP64 form of this code (itself 1e-12 parity with the oracle)"}
+
+
+def e2e_run(torch, ns, n, W, steps, device):
+    """Same metric through the public API with host buffers: every step uploads
+    its inputs from pinned host memory, steps, and reads the total energy."""
+    pinned = torch.empty((5,) + W.shape[1:], dtype=torch.float64, pin_memory=True)
+    pinned.numpy()[...] = W
+    host = pinned.numpy()
+    with ns.Solver(make_params(ns, n, "fp32acc64"), device=device) as s:
+        stream = torch.cuda.ExternalStream(s.stream_handle())
+        s.upload_primitive(host)
+        s.step(1)
+        s.compute_total_energy()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(steps):
+            s.upload_primitive(host)
+            s.step(1)
+            s.compute_total_energy()
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1)
+    h2d = 5 * W[0].size * 8
+    d2h = 12 * 8
+    return {"value": steps / (ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "wall_steps_per_s": steps / wall,
+            "path": "Solver.upload_primitive(pinned host) + step(1) + compute_total_energy"}
+
+
+def ncu_traffic():
+    """DRAM bytes per launch per kernel class from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def our_arm(args, rank, world, local):
+    import torch
+    use_cuda = torch.cuda.is_available()
+    if not use_cuda:
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    dist = dist_init(world, use_cuda)
+    import ns3d_cpp_b200 as ns
+    n = args.n
+    W = workload_input(n)
+    ncell = n ** 3
+    peak, peak_kind = measured_peaks()
+
+    # --- the headline form: FP32 stencils, FP64 accumulation ---
+    with ns.Solver(make_params(ns, n, "fp32acc64"), device=local) as s:
+        s.upload_primitive(W)
+        with ClockSampler(local) as clk:
+            ms, launches, prof = timed_steps(torch, s, args.steps, args.warmup, dist, use_cuda)
+        clocks = clk.summary()
+    ms_max = dist_max(dist, ms, use_cuda)
+    value = world * args.steps / (ms_max / 1e3)
+
+    # --- the plain FP64 form on the same workload ---
+    k64 = max(3, args.steps // 3)
+    with ns.Solver(make_params(ns, n, "fp64"), device=local) as s:
+        s.upload_primitive(W)
+        ms64, _, prof64 = timed_steps(torch, s, k64, max(3, args.warmup // 2), dist, use_cuda)
+    ms64_max = dist_max(dist, ms64, use_cuda)
+    fp64_sps = world * k64 / (ms64_max / 1e3)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    errors = error_run(ns, n, W, args.err_steps, local) if args.err_steps > 0 else None
+    e2e = e2e_run(torch, ns, n, W, args.e2e_steps, local)
+
+    # dominant kernel roofline (per launch, CUDA-event timed in the timed region)
+    rsize = 4
+    kern = {}
+    for cls, (kms, cnt) in prof.items():
+        if cnt:
+            b = kernel_bytes_per_cell(cls, rsize) * ncell
+            kern[cls] = {"launches": cnt, "ms_total": kms, "ms_per_launch": kms / cnt,
+                         "share": kms / max(1e-9, sum(v[0] for v in prof.values())),
+                         "alg_bytes_per_launch": b,
+                         "achieved_gbs": b / (kms / cnt / 1e3) / 1e9 if b else None}
+    dom = max((c for c in kern if c != "other"), key=lambda c: kern[c]["ms_total"])
+    traffic = ncu_traffic().get(f"fp32acc64/{dom}")
+    ach = kern[dom]["achieved_gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
+                "alg_bytes_per_cell": kernel_bytes_per_cell(dom, rsize)}
+    step_ach = STEP_BYTES_PER_CELL * ncell * (value / world) / 1e9
+    roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s",
+                     "frac": step_ach / peak, "alg_bytes_per_cell_step": STEP_BYTES_PER_CELL}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample_steps, n)
+
+    line = {
+        "metric": METRIC,
+        "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 stencils / fp64 accumulate",
+        "data": "synthetic: seeded isotropic turbulence (numpy), inputs resident in HBM",
+        "config": {"workload": f"isotropic turbulence {n}^3, Mach_t 0.5, Re 1000, SW+WENO5, C8th",
+                   "n": n, "cells": ncell, "precision": "fp32acc64",
+                   "l2": f"inputs larger than L2: {6 * ncell * 8 / 1e6:.0f} MB per state buffer",
+                   "parallelism": f"replicas x{world}"},
+        "gcell_per_s": value * ncell / 1e9,
+        "fp64": {"steps_per_s": fp64_sps, "gcell_per_s": fp64_sps * ncell / 1e9,
+                 "steps": k64, "ms_per_step": ms64_max / k64,
+                 "kernels_ms_per_launch": {c: (v[0] / v[1] if v[1] else None)
+                                           for c, v in prof64.items()}},
+        "fp32_over_fp64": value / fp64_sps,
+        "errors_fp32_vs_fp64": errors,
+        "roofline": roofline, "roofline_step": roofline_step, "kernels": kern,
+        "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------
+# the reference CPU path
+# ----------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    """One replica: the reference (or the oracle port) on a periodic sub-box.
+    Runs in a spawned process; returns seconds per RK3 step."""
+    kind, n, steps, warm = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from ns3d_cpp_b200 import initial
+    w = WORKLOAD
+    two_pi = "6.283185307179586"
+    cfg = dict(gamma=w["gamma"], Pr=w["Pr"], Ma=w["Ma"], Re=w["Re"], cfl=w["cfl"], dt_fixed=-1,
+               fvs_type="StagerWarming", recon="WENO5", vis_scheme="C8th",
+               global_nx=n, global_ny=n, global_nz=n, Lx=two_pi, Ly=two_pi, Lz=two_pi,
+               Post_BasicField="False", IsotropicAnalyse="False", monitor_Res="False",
+               monitor_Energy="False")
+    W = initial.isotropic(n, mach_t=w["mach_t"], Ma=w["Ma"], gamma=w["gamma"], k0=w["k0"],
+                          seed=w["seed"])
+    if kind == "reference":
+        r = oracle.Ref(cfg)
+        r.set_primitive(W)
+        for _ in range(warm):
+            r.cfl_step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r.cfl_step()
+        return (time.perf_counter() - t0) / steps
+    os.environ["OMP_NUM_THREADS"] = "1"
+    o = oracle.Oracle(cfg)
+    for _ in range(warm):
+        W, _, _ = o.cfl_step(W)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        W, _, _ = o.cfl_step(W)
+    return (time.perf_counter() - t0) / steps
+
+
+def run_cpu(steps: int, warm: int, n_equiv: int):
+    """Reference path on all host cores as independent single-rank replicas
+    (the reference's one-rank build; no MPI on this host). Returns a dict."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    kind = "reference" if oracle.have_ref() else "port"
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        per_step = pool.map(_cpu_worker, [(kind, CPU_SAMPLE_N, steps, warm)] * cores)
+    wall = time.perf_counter() - t0
+    cells = CPU_SAMPLE_N ** 3
+    cell_rate = sum(cells / t for t in per_step)
+    return {"value": cell_rate / n_equiv ** 3, "unit": "steps/s", "cores": cores, "kind": kind,
+            "cell_updates_per_s": cell_rate, "s_per_step_one_core": statistics.mean(per_step),
+            "sample": (f"{cores} concurrent single-rank replicas (one per host core, replicas, "
+                       f"not one domain), each {steps} RK3 step(s) of the same scheme on a "
+                       f"{CPU_SAMPLE_N}^3 periodic isotropic box after {warm} warm-up; "
+                       f"steps/s scaled to {n_equiv}^3 by cell count; wall {wall:.1f} s")}
+
+
+def cpu_baseline(steps: int, n: int):
+    try:
+        return run_cpu(steps, 0, n)
+    except Exception as e:  # reported, never fatal for the GPU line
+        return {"value": None, "error": str(e)}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    res = run_cpu(args.steps, args.warmup, args.n)
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": "steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded isotropic turbulence (numpy)",
+            "config": {"workload": (f"isotropic turbulence {args.n}^3, Mach_t 0.5, Re 1000, "
+                                    "SW+WENO5, C8th"), "n": args.n},
+            "cpu_baseline": {"value": res["value"], "unit": "steps/s", "cores": res["cores"],
+                             "kind": res["kind"], "sample": res["sample"]},
+            "e2e": {"value": res["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "cell_updates_per_s": res["cell_updates_per_s"]}
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--err-steps", type=int, default=500)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(3, args.warmup)
+    rank, world, local = env_rank()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    our_arm(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * ns3d_gpu.h -- C ABI of the B200 implementation of ns3d_cpp's right-hand side
+ * and RK3 time-step loop (3D compressible Navier-Stokes, periodic box).
+ *
+ * Plain C: opaque handle, POD parameter struct, host pointers and sizes. Every
+ * function returns an ns3d_status (0 = success). One context owns one device
+ * copy of the state and one CUDA stream; calls on one context must not overlap
+ * from several threads.
+ *
+ * Each entry point names the reference function it replaces (file:line in
+ * wylx-2/ns3d_cpp). The reference's C++ signatures (compute_rhs,
+ * runge_kutta_3, compute_timestep, time_advance over Field3D) are provided on
+ * top of this ABI by the shim described in INTEGRATION.md.
+ *
+ * Arrays cross the boundary in one of two layouts (x fastest in both):
+ *   NS3D_LAYOUT_INTERIOR  nx*ny*nz, a[(k*ny + j)*nx + i]
+ *   NS3D_LAYOUT_GHOSTED   the reference Field3D layout, sx*sy*sz with
+ *                         s = n + 2*ghost_layers, idx3 (field_structures.h:63)
+ */
+#ifndef NS3D_GPU_H
+#define NS3D_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ns3d_status {
+    NS3D_OK = 0,
+    NS3D_ERR_INVALID = 1,      /* bad argument or configuration */
+    NS3D_ERR_UNSUPPORTED = 2,  /* valid in the reference, not built here */
+    NS3D_ERR_CUDA = 3,         /* CUDA runtime / cuFFT failure */
+    NS3D_ERR_NONPHYSICAL = 4,  /* rho, p or T <= 0 after a step (range_kutta.cpp:149-162) */
+    NS3D_ERR_FILE = 5,         /* solver.in cannot be opened (initialization.cpp:206-209) */
+    NS3D_ERR_DT = 6,           /* dt <= 1e-12: time_advance stops (maincycle.cpp:46-52) */
+    NS3D_ERR_NOMEM = 7,        /* device allocation failed */
+    NS3D_ERR_TIMEOUT = 8       /* a bounded device-side wait gave up */
+} ns3d_status;
+
+/* Enumerations keep the reference's enum order (field_structures.h:112-145). */
+enum { NS3D_FVS_STEGER_WARMING = 0, NS3D_FVS_LAX_FRIEDRICHS = 1 };
+enum {
+    NS3D_RECON_WENO5 = 0, NS3D_RECON_WCNS = 1, NS3D_RECON_LINEAR = 2, NS3D_RECON_MDCD = 3,
+    NS3D_RECON_MDCD_HYBRID = 4, NS3D_RECON_UPWIND_7TH = 5, NS3D_RECON_UD7L = 6
+};
+enum { NS3D_VIS_C8TH = 0, NS3D_VIS_C6TH = 1, NS3D_VIS_C4TH = 2 };
+enum { NS3D_BC_PERIODIC = 0, NS3D_BC_WALL = 1, NS3D_BC_SYMMETRY = 2, NS3D_BC_OUTFLOW = 3,
+       NS3D_BC_INFLOW = 4 };
+/* Precision forms. FP64: every operation in double, operation order of the
+ * reference, no FMA contraction (1e-12 parity form). FP32_ACC64: splitting,
+ * reconstruction and viscous stencils in float; state, RK3 stage accumulation
+ * and all reductions in double. */
+enum { NS3D_PREC_FP64 = 0, NS3D_PREC_FP32_ACC64 = 1 };
+enum { NS3D_LAYOUT_INTERIOR = 0, NS3D_LAYOUT_GHOSTED = 1 };
+
+/* SolverParams + GridDesc + the periodicity of CartDecomp
+ * (field_structures.h:32-37, 85-166). */
+typedef struct ns3d_params {
+    /* physical (SolverParams) */
+    double gamma, Pr, Ma, Re;
+    /* time stepping */
+    double cfl, dt_fixed;
+    /* schemes */
+    int fvs_type, recon, vis_scheme, char_recon;
+    double mdcd_diss, mdcd_disp, ud7l_alpha;
+    /* grid (GridDesc) */
+    int global_nx, global_ny, global_nz;
+    double x0, y0, z0, Lx, Ly, Lz;
+    /* boundary types xmin, xmax, ymin, ymax, zmin, zmax */
+    int bc[6];
+    /* simulation control */
+    int max_steps, monitor_Stepfreq;
+    double output_Timefreq, TotalTime;
+    int post_basicfield, isotropic_analyse, monitor_res, monitor_energy;
+    /* derived by ns3d_params_derive (initialization.cpp:312-377) */
+    double Cv, Cp, Rgas, mu, dx, dy, dz;
+    int stencil, ghost_layers;
+    int periods[3];
+    /* extensions; the defaults reproduce the reference */
+    double sw_entropy_eps;          /* |l| -> sqrt(l^2+eps^2) in Steger-Warming (README.md:177-180); 0 */
+    double sutherland_s_over_tref;  /* S/Tref of get_mu; 110.4/288.15 (field_structures.h:100) */
+    int precision;                  /* NS3D_PREC_*; default FP64 */
+    int reserved[7];
+} ns3d_params;
+
+typedef struct ns3d_ctx ns3d_ctx;
+
+/* Turbulence statistics of compute_turbulence_statistics (ana_isotropic.cpp:196-314),
+ * the spectrum taken at full precision (the reference re-reads it from a 6-digit file). */
+typedef struct ns3d_turb_stats {
+    double kinetic_energy;  /* <0.5|u|^2> */
+    double tke;             /* 0.5 (var u + var v + var w) */
+    double u_rms;           /* sqrt(<|u|^2>/3) */
+    double dissipation;     /* 2 nu sum_k k^2 E(k), nu = <mu(T)>/<rho> */
+    double nu, mean_mu, mean_rho;
+    double mach_t;          /* sqrt(2 KE) / <c> */
+    double total_energy;    /* sum 0.5 rho |u|^2 dV (compute_total_energy, postprocess.cpp:103) */
+    double reserved[7];
+} ns3d_turb_stats;
+
+/* ---- parameters ---------------------------------------------------------- */
+
+/* SolverParams() defaults plus the parser's grid defaults (16^3, origin 0). */
+ns3d_status ns3d_params_default(ns3d_params *p);
+/* read_solver_params_from_file (initialization.cpp:199-380): key = value, '#'
+ * comments, case-insensitive keys, unknown keys ignored; then derives. Also
+ * accepts the extension keys sw_entropy_eps, sutherland_s_over_tref and
+ * precision (fp64 | fp32acc64). */
+ns3d_status ns3d_params_from_file(const char *path, ns3d_params *p);
+/* The derivation step alone (initialization.cpp:312-377). */
+ns3d_status ns3d_params_derive(ns3d_params *p);
+/* sizeof(ns3d_params) and sizeof(ns3d_turb_stats), for bindings to check
+ * their struct layout (no reference counterpart). */
+size_t ns3d_params_size(void);
+size_t ns3d_turb_stats_size(void);
+
+/* ---- context ------------------------------------------------------------- */
+
+/* Field3D::allocate (field_structures.h:225) on `device`, interior-only and
+ * resident in HBM. Rejects non-periodic boundaries, char_recon and WCNS with
+ * NS3D_ERR_UNSUPPORTED. */
+ns3d_status ns3d_create(const ns3d_params *p, int device, ns3d_ctx **out);
+ns3d_status ns3d_destroy(ns3d_ctx *ctx);
+/* Last error message of this context (static string for ctx == NULL). */
+const char *ns3d_last_error(const ns3d_ctx *ctx);
+ns3d_status ns3d_get_params(const ns3d_ctx *ctx, ns3d_params *out);
+/* Bytes of device memory the context holds. */
+ns3d_status ns3d_device_bytes(const ns3d_ctx *ctx, size_t *bytes);
+ns3d_status ns3d_synchronize(ns3d_ctx *ctx);
+
+/* ---- state transfer (host pointers) ---------------------------------------- */
+
+/* Initial condition path: interior primitives, then apply_boundary +
+ * primitiveToConserved (main.cpp:67-71). Also records U0 (recordConservedTo0). */
+ns3d_status ns3d_upload_primitive(ns3d_ctx *ctx, const double *rho, const double *u,
+                                  const double *v, const double *w, const double *p,
+                                  int layout);
+/* Conserved state: conservedToPrimitive + apply_boundary + primitiveToConserved
+ * (range_kutta.cpp:117-119). Also records U0. */
+ns3d_status ns3d_upload_conserved(ns3d_ctx *ctx, const double *rho, const double *rhou,
+                                  const double *rhov, const double *rhow, const double *E,
+                                  int layout);
+/* Primitives (rho,u,v,w,p) as Field3D holds them after a step; optional T, c
+ * (NULL to skip). Ghost faces hold periodic images; edges/corners hold the
+ * values a Field3D keeps there (rho=1, others 0). */
+ns3d_status ns3d_download_primitive(ns3d_ctx *ctx, double *rho, double *u, double *v,
+                                    double *w, double *p, double *T, double *c, int layout);
+/* Conserved (rho, rhou, rhov, rhow, E) = primitiveToConserved of the state. */
+ns3d_status ns3d_download_conserved(ns3d_ctx *ctx, double *rho, double *rhou, double *rhov,
+                                    double *rhow, double *E, int layout);
+
+/* ---- the hot path ----------------------------------------------------------- */
+
+/* Field3D::recordConservedTo0 (field_structures.h:454). */
+ns3d_status ns3d_record_conserved0(ns3d_ctx *ctx);
+/* compute_rhs (range_kutta.cpp:11-99) of the current state; copies the five
+ * rhs arrays to the host pointers (any may be NULL). */
+ns3d_status ns3d_compute_rhs(ns3d_ctx *ctx, double *rhs_rho, double *rhs_rhou,
+                             double *rhs_rhov, double *rhs_rhow, double *rhs_E, int layout);
+/* compute_timestep (timestep.cpp:5-33): cfl * min over cells. */
+ns3d_status ns3d_compute_timestep(ns3d_ctx *ctx, double *dt);
+/* runge_kutta_3 (range_kutta.cpp:102-163) with the recorded U0; returns
+ * NS3D_ERR_NONPHYSICAL (instead of MPI_Abort) if rho, p or T <= 0 afterwards. */
+ns3d_status ns3d_runge_kutta_3(ns3d_ctx *ctx, double dt);
+/* time_advance (maincycle.cpp:7-112) without monitor output: up to `max_steps`
+ * steps of recordConservedTo0 + dt (CFL or dt_fixed) + the clipping to
+ * TotalTime and output times + runge_kutta_3, all on the device with no host
+ * round trip per step. `time` is in/out (current_time); `steps_done` receives
+ * the number of completed steps. Stops early exactly where time_advance does. */
+ns3d_status ns3d_time_advance(ns3d_ctx *ctx, int max_steps, double *time, int *steps_done);
+/* `nsteps` RK3 steps with a CFL (or fixed) dt each, no clipping: the bench step. */
+ns3d_status ns3d_step(ns3d_ctx *ctx, int nsteps);
+/* dt of the last step taken on the device. */
+ns3d_status ns3d_last_dt(ns3d_ctx *ctx, double *dt);
+
+/* ---- instrumentation (no reference counterpart) -------------------------- */
+
+/* Kernel classes timed by ns3d_profile. */
+enum {
+    NS3D_KERNEL_SWEEP_X = 0, NS3D_KERNEL_SWEEP_Y = 1, NS3D_KERNEL_SWEEP_Z = 2,
+    NS3D_KERNEL_VISC_FLUX = 3, NS3D_KERNEL_UPDATE = 4, NS3D_KERNEL_OTHER = 5,
+    NS3D_KERNEL_CLASSES = 6
+};
+/* The cudaStream_t every kernel of this context is launched on. */
+ns3d_status ns3d_get_stream(ns3d_ctx *ctx, void **stream);
+/* enable != 0: reset and start recording a CUDA event pair around every
+ * launch, per kernel class; enable == 0: stop recording. */
+ns3d_status ns3d_profile(ns3d_ctx *ctx, int enable);
+/* Summed device milliseconds and launch counts per class since the last
+ * ns3d_profile(ctx, 1); arrays of NS3D_KERNEL_CLASSES entries. Synchronizes. */
+ns3d_status ns3d_profile_read(ns3d_ctx *ctx, double *ms, long long *launches);
+/* Kernels this context has launched since creation. */
+ns3d_status ns3d_launch_count(const ns3d_ctx *ctx, long long *count);
+
+/* ---- reductions ----------------------------------------------------------- */
+
+/* compute_total_energy (postprocess.cpp:103-128): sum 0.5 rho |u|^2 dx dy dz. */
+ns3d_status ns3d_total_energy(ns3d_ctx *ctx, double *etot);
+/* compute_energy_spectrum (EnergySpectrum.cpp:62-125): E(k), k = 0..nbins-1,
+ * nbins <= 2*global_nx + 1; transform of u,v,w scaled by 1/N, shells by floor(|k|). */
+ns3d_status ns3d_energy_spectrum(ns3d_ctx *ctx, double *Ek, int nbins);
+/* compute_turbulence_statistics, KE and dissipation parts (ana_isotropic.cpp:241-303). */
+ns3d_status ns3d_turbulence_stats(ns3d_ctx *ctx, ns3d_turb_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NS3D_GPU_H */

@@ -1,0 +1,877 @@
+// C ABI implementation: context, device buffers, transfers and the
+// sequencing of the stage kernels. Declarations and reference citations are
+// in include/ns3d_gpu.h.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ns3d_gpu.h"
+#define NS3D_API_KERNELS
+#include "ns3d_launch.cuh"
+
+using namespace ns3d;
+
+namespace ns3d {
+// explicit instantiations live in ns3d_fp64.cu / ns3d_fp32.cu
+extern template cudaError_t launch_sweep<double>(const LaunchCfg&, int, StateView, double*, const Ctrl*);
+extern template cudaError_t launch_visc_flux<double>(const LaunchCfg&, StateView, double*, const Ctrl*);
+extern template cudaError_t launch_update<double>(const LaunchCfg&, int, StateView, StateView,
+                                                  const double*, const double*, StateOut, Ctrl*);
+extern template cudaError_t launch_rhs_out<double>(const LaunchCfg&, const double*, const double*, double*);
+extern template cudaError_t launch_sweep<float>(const LaunchCfg&, int, StateView, float*, const Ctrl*);
+extern template cudaError_t launch_visc_flux<float>(const LaunchCfg&, StateView, float*, const Ctrl*);
+extern template cudaError_t launch_update<float>(const LaunchCfg&, int, StateView, StateView,
+                                                 const float*, const float*, StateOut, Ctrl*);
+extern template cudaError_t launch_rhs_out<float>(const LaunchCfg&, const float*, const float*, double*);
+}  // namespace ns3d
+
+struct ns3d_ctx {
+    ns3d_params p;
+    LaunchCfg L;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    long long n = 0;
+    double* wmem = nullptr;      // 3 state buffers x 6 arrays x n
+    int cur = 0, rec = 0;        // current state buffer, recorded (U0) buffer
+    void* tacc = nullptr;        // 5 n (R)
+    void* fv = nullptr;          // 9 n (R)
+    size_t rsize = 8;            // sizeof(R)
+    Ctrl* ctrl = nullptr;
+    Ctrl* ctrl_host = nullptr;   // pinned mirror
+    double* sums_part = nullptr; // partial sums
+    double* sums_out = nullptr;
+    int sums_blocks = 0;
+    bool dtmin_valid = false;
+    double time = 0.0, out_next = 0.0;
+    // spectrum
+    cufftHandle fft = 0;
+    bool fft_ready = false;
+    cufftDoubleComplex* spec = nullptr;
+    double* bins = nullptr;
+    // instrumentation
+    long long launches = 0;
+    bool prof_on = false;
+    struct ProfRec { int cls; cudaEvent_t a, b; };
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::string err;
+};
+
+namespace {
+
+const char* kStaticErr = "invalid context";
+
+ns3d_status fail(ns3d_ctx* c, ns3d_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+#define NS3D_CK(call)                                                                     \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(ctx, NS3D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+double* warr(ns3d_ctx* c, int buf, int a) { return c->wmem + ((long long)buf * 6 + a) * c->n; }
+
+cudaEvent_t pool_event(ns3d_ctx* c) {
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+
+// Launch `nk` kernels through `f` (returns cudaError_t) as kernel class `cls`:
+// counted, and bracketed by an event pair when profiling is on.
+template <class F>
+ns3d_status launch(ns3d_ctx* ctx, int cls, int nk, F&& f) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (ctx->prof_on) {
+        a = pool_event(ctx);
+        b = pool_event(ctx);
+        if (a && b) cudaEventRecord(a, ctx->stream);
+    }
+    const cudaError_t e = f();
+    if (e != cudaSuccess) return fail(ctx, NS3D_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    if (a && b) {
+        cudaEventRecord(b, ctx->stream);
+        ctx->prof.push_back({cls, a, b});
+    }
+    ctx->launches += nk;
+    return NS3D_OK;
+}
+
+#define NS3D_LAUNCH(cls, nk, expr)                                                   \
+    do {                                                                             \
+        ns3d_status s_ = launch(ctx, (cls), (nk), [&]() -> cudaError_t { expr; return cudaGetLastError(); }); \
+        if (s_ != NS3D_OK) return s_;                                                \
+    } while (0)
+
+StateView view(ns3d_ctx* c, int buf) {
+    return StateView{warr(c, buf, 0), warr(c, buf, 1), warr(c, buf, 2),
+                     warr(c, buf, 3), warr(c, buf, 4), warr(c, buf, 5)};
+}
+StateOut outv(ns3d_ctx* c, int buf) {
+    return StateOut{warr(c, buf, 0), warr(c, buf, 1), warr(c, buf, 2),
+                    warr(c, buf, 3), warr(c, buf, 4), warr(c, buf, 5)};
+}
+
+int recon_kind(int recon) {
+    switch (recon) {
+    case NS3D_RECON_WENO5: return RC_WENO5;
+    case NS3D_RECON_LINEAR: return RC_LINEAR;
+    case NS3D_RECON_MDCD: return RC_LIN6;
+    case NS3D_RECON_MDCD_HYBRID: return RC_MDCD_HYBRID;
+    case NS3D_RECON_UPWIND_7TH: case NS3D_RECON_UD7L: return RC_LIN8;
+    default: return -1;
+    }
+}
+
+// Linear reconstruction coefficients evaluated with the reference's own
+// expressions (reconstruction.cpp:126-135, 227-249).
+void linear_coefficients(const ns3d_params& p, double lin[8]) {
+    for (int m = 0; m < 8; ++m) lin[m] = 0.0;
+    if (p.recon == NS3D_RECON_MDCD || p.recon == NS3D_RECON_MDCD_HYBRID) {
+        const double diss = p.mdcd_diss, disp = p.mdcd_disp;
+        lin[0] = (1.0 / 2.0 * disp + 1.0 / 2.0 * diss);
+        lin[1] = (-3.0 / 2.0 * disp - 5.0 / 2.0 * diss - 1.0 / 12.0);
+        lin[2] = (7.0 / 12.0 + disp + 5.0 * diss);
+        lin[3] = (7.0 / 12.0 + disp - 5.0 * diss);
+        lin[4] = (-3.0 / 2.0 * disp + 5.0 / 2.0 * diss - 1.0 / 12.0);
+        lin[5] = (1.0 / 2.0 * disp - 1.0 / 2.0 * diss);
+    } else if (p.recon == NS3D_RECON_UPWIND_7TH) {
+        // a0*s0 + ... with a2, a5 negative: x - c*s == x + (-c)*s exactly, and
+        // the a7*s7 = 0*s7 term adds a signed zero, which changes nothing.
+        lin[0] = -1.0 / 140.0;
+        lin[1] = 5.0 / 84.0;
+        lin[2] = -(101.0 / 420.0);
+        lin[3] = 319.0 / 420.0;
+        lin[4] = 107.0 / 210.0;
+        lin[5] = -(19.0 / 210.0);
+        lin[6] = 1.0 / 105.0;
+        lin[7] = 0.0;
+    } else if (p.recon == NS3D_RECON_UD7L) {
+        const double alpha = p.ud7l_alpha;
+        lin[0] = -3.0 / 420.0 * alpha - 3.0 / 840.0 * (1.0 - alpha);
+        lin[1] = 25.0 / 420.0 * alpha + 29.0 / 840.0 * (1.0 - alpha);
+        lin[2] = -101.0 / 420.0 * alpha - 139.0 / 840.0 * (1.0 - alpha);
+        lin[3] = 319.0 / 420.0 * alpha + 533.0 / 840.0 * (1.0 - alpha);
+        lin[4] = 214.0 / 420.0 * alpha + 533.0 / 840.0 * (1.0 - alpha);
+        lin[5] = -38.0 / 420.0 * alpha - 139.0 / 840.0 * (1.0 - alpha);
+        lin[6] = 4.0 / 420.0 * alpha + 29.0 / 840.0 * (1.0 - alpha);
+        lin[7] = (-3.0 / 840.0) * (1.0 - alpha);
+    }
+}
+
+// ---- small kernels of the API layer (FP64, this TU is built with -fmad=false)
+
+// primitiveToConserved's density clamp and T after an upload of primitives.
+__global__ void k_prim_finish(DevParams P, StateOut W) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= P.n) return;
+    double rr = W.rho[id];
+    if (rr <= 0.0) { rr = 1e-12; W.rho[id] = rr; }
+    W.T[id] = W.p[id] / (rr * P.Rgas);
+}
+
+// conservedToPrimitive (+ T) of an uploaded conserved state held in `U`.
+__global__ void k_cons2prim(DevParams P, const double* __restrict__ U, StateOut W) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= P.n) return;
+    const long long n = P.n;
+    double rr = U[id];
+    if (rr <= 0.0) rr = 1e-12;
+    const double u = U[n + id] / rr, v = U[2 * n + id] / rr, w = U[3 * n + id] / rr;
+    const double kinetic = 0.5 * (u * u + v * v + w * w);
+    const double e_internal = U[4 * n + id] / rr - kinetic;
+    const double p = (P.gamma - 1.0) * rr * e_internal;
+    W.rho[id] = rr; W.u[id] = u; W.v[id] = v; W.w[id] = w; W.p[id] = p;
+    W.T[id] = p / (rr * P.Rgas);
+}
+
+// primitiveToConserved of the state into 5 blocks; c into `c` when non-null.
+__global__ void k_prim2cons(DevParams P, StateView W, double* __restrict__ U, double* __restrict__ c) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= P.n) return;
+    double Uc[5];
+    prim2cons_cell(W, id, P.gamma, Uc);
+    for (int q = 0; q < 5; ++q) U[q * P.n + id] = Uc[q];
+    if (c) c[id] = sqrt(P.gamma * W.p[id] / Uc[0]);
+}
+
+// Shell binning of |u_hat|^2 (EnergySpectrum.cpp:99-125) from a D2Z transform
+// (x half-spectrum): modes strictly inside the half-space count twice.
+__global__ void k_spectrum_bin(const cufftDoubleComplex* __restrict__ X, int nx, int ny, int nz,
+                               double scale, int nbins, double* __restrict__ bins) {
+    extern __shared__ double sb[];
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) sb[b] = 0.0;
+    __syncthreads();
+    const int nxh = nx / 2 + 1;
+    const long long total = (long long)nxh * ny * nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int ic = (int)(t % nxh);
+        const long long r = t / nxh;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+        const int k1 = ic;
+        const int k2 = j <= ny / 2 ? j : j - ny;
+        const int k3 = k <= nz / 2 ? k : k - nz;
+        const int kk = (int)sqrt(1.0 * (k1 * k1 + k2 * k2 + k3 * k3));
+        const double re = X[t].x * scale, im = X[t].y * scale;
+        double e = 0.5 * (re * re + im * im);
+        const bool self_conj = (ic == 0) || ((nx % 2 == 0) && ic == nx / 2);
+        if (!self_conj) e *= 2.0;
+        if (kk < nbins) atomicAdd(&sb[kk], e);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        if (sb[b] != 0.0) atomicAdd(&bins[b], sb[b]);
+}
+
+ns3d_status validate(const ns3d_params* p, std::string& msg) {
+    for (int f = 0; f < 6; ++f)
+        if (p->bc[f] != NS3D_BC_PERIODIC) {
+            msg = "only periodic boundaries are built (boundary.cpp:56-207 is out of scope)";
+            return NS3D_ERR_UNSUPPORTED;
+        }
+    if (p->char_recon) {
+        msg = "char_recon (InviscousFlux_new.cpp:165-437) is not built";
+        return NS3D_ERR_UNSUPPORTED;
+    }
+    if (recon_kind(p->recon) < 0) {
+        msg = "reconstruction WCNS has no implementation in the reference either";
+        return NS3D_ERR_UNSUPPORTED;
+    }
+    if (p->fvs_type != NS3D_FVS_STEGER_WARMING && p->fvs_type != NS3D_FVS_LAX_FRIEDRICHS) {
+        msg = "unknown fvs_type";
+        return NS3D_ERR_INVALID;
+    }
+    if (p->vis_scheme < NS3D_VIS_C8TH || p->vis_scheme > NS3D_VIS_C4TH) {
+        msg = "unknown vis_scheme";
+        return NS3D_ERR_INVALID;
+    }
+    if (p->global_nx < 8 || p->global_ny < 8 || p->global_nz < 8) {
+        msg = "each extent must be at least 8 cells";
+        return NS3D_ERR_INVALID;
+    }
+    if ((long long)p->global_nx * p->global_ny * p->global_nz > (1ll << 31)) {
+        msg = "grid larger than 2^31 cells";
+        return NS3D_ERR_INVALID;
+    }
+    if (p->precision != NS3D_PREC_FP64 && p->precision != NS3D_PREC_FP32_ACC64) {
+        msg = "unknown precision";
+        return NS3D_ERR_INVALID;
+    }
+    if (!(p->gamma > 1.0) || !(p->Ma > 0.0) || !(p->Re > 0.0) || !(p->Pr > 0.0)) {
+        msg = "gamma > 1, Ma > 0, Re > 0 and Pr > 0 are required";
+        return NS3D_ERR_INVALID;
+    }
+    return NS3D_OK;
+}
+
+inline unsigned blocks_for(long long n, int th) { return (unsigned)((n + th - 1) / th); }
+
+ns3d_status reset_ctrl(ns3d_ctx* ctx) {
+    Ctrl h{};
+    h.dtmin_bits = 0;
+    std::memcpy(&h.dtmin_bits, &CFL_INIT, sizeof(double));
+    h.time = ctx->time;
+    h.out_next = ctx->out_next;
+    h.bad_cell = ctx->n;
+    *ctx->ctrl_host = h;
+    NS3D_CK(cudaMemcpyAsync(ctx->ctrl, ctx->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    return NS3D_OK;
+}
+
+ns3d_status read_ctrl(ns3d_ctx* ctx) {
+    NS3D_CK(cudaMemcpyAsync(ctx->ctrl_host, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+// The RHS pieces of the current state (sweeps + viscous flux) into tacc/fv.
+template <class R>
+ns3d_status rhs_parts_t(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl) {
+    R* tacc = (R*)ctx->tacc;
+    for (int dir = 0; dir < 3; ++dir)
+        NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X + dir, 1, launch_sweep<R>(ctx->L, dir, W, tacc, ctrl));
+    NS3D_LAUNCH(NS3D_KERNEL_VISC_FLUX, 1, launch_visc_flux<R>(ctx->L, W, (R*)ctx->fv, ctrl));
+    return NS3D_OK;
+}
+
+// The RHS pieces of the current state (sweeps + viscous flux) into tacc/fv.
+ns3d_status launch_rhs_parts(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl) {
+    return ctx->p.precision == NS3D_PREC_FP64 ? rhs_parts_t<double>(ctx, W, ctrl)
+                                              : rhs_parts_t<float>(ctx, W, ctrl);
+}
+
+template <class R>
+ns3d_status update_t(ns3d_ctx* ctx, int stage, StateView Wc, StateView W0, int bn) {
+    NS3D_LAUNCH(NS3D_KERNEL_UPDATE, 1,
+                launch_update<R>(ctx->L, stage, Wc, W0, (const R*)ctx->tacc, (const R*)ctx->fv,
+                                 outv(ctx, bn), ctx->ctrl));
+    return NS3D_OK;
+}
+
+ns3d_status launch_stage(ns3d_ctx* ctx, int stage, int bc, int b0, int bn) {
+    const StateView Wc = view(ctx, bc), W0 = view(ctx, b0);
+    ns3d_status s = launch_rhs_parts(ctx, Wc, ctx->ctrl);
+    if (s != NS3D_OK) return s;
+    return ctx->p.precision == NS3D_PREC_FP64 ? update_t<double>(ctx, stage, Wc, W0, bn)
+                                              : update_t<float>(ctx, stage, Wc, W0, bn);
+}
+
+// One runge_kutta_3 on the device with dt from ctrl->dt. Buffer rotation keeps
+// the recorded state intact, so U0 stays valid exactly as rho0.. do.
+ns3d_status enqueue_rk3(ns3d_ctx* ctx) {
+    int a = ctx->cur, r = ctx->rec, x, y;
+    if (a == r) {
+        x = (a + 1) % 3;
+        y = (a + 2) % 3;
+        ns3d_status s;
+        if ((s = launch_stage(ctx, 1, a, r, x)) != NS3D_OK) return s;
+        if ((s = launch_stage(ctx, 2, x, r, y)) != NS3D_OK) return s;
+        if ((s = launch_stage(ctx, 3, y, r, x)) != NS3D_OK) return s;
+        ctx->cur = x;
+    } else {
+        const int z = 3 - a - r;
+        ns3d_status s;
+        if ((s = launch_stage(ctx, 1, a, r, z)) != NS3D_OK) return s;
+        if ((s = launch_stage(ctx, 2, z, r, a)) != NS3D_OK) return s;
+        if ((s = launch_stage(ctx, 3, a, r, z)) != NS3D_OK) return s;
+        ctx->cur = z;
+    }
+    return NS3D_OK;
+}
+
+ns3d_status enqueue_cfl(ns3d_ctx* ctx) {
+    NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                (k_cfl<<<blocks_for(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->L.P, view(ctx, ctx->cur),
+                                                                       ctx->ctrl)));
+    ctx->dtmin_valid = true;
+    return NS3D_OK;
+}
+
+// Host layout conversions ---------------------------------------------------
+
+void gather_interior(const ns3d_params& p, const double* src, double* dst) {
+    const int g = p.ghost_layers;
+    const long long sx = p.global_nx + 2 * g, sy = p.global_ny + 2 * g;
+    long long q = 0;
+    for (int k = 0; k < p.global_nz; ++k)
+        for (int j = 0; j < p.global_ny; ++j) {
+            const double* row = src + ((k + g) * sy + (j + g)) * sx + g;
+            std::memcpy(dst + q, row, sizeof(double) * p.global_nx);
+            q += p.global_nx;
+        }
+}
+
+// Interior -> Field3D layout: face ghosts get periodic images (apply_boundary),
+// edges and corners get `fill` (what Field3D keeps there).
+void scatter_ghosted(const ns3d_params& p, const double* src, double* dst, double fill) {
+    const int g = p.ghost_layers, nx = p.global_nx, ny = p.global_ny, nz = p.global_nz;
+    const long long sx = nx + 2 * g, sy = ny + 2 * g, sz = nz + 2 * g;
+    for (long long t = 0; t < sx * sy * sz; ++t) dst[t] = fill;
+    auto wrapi = [](int a, int n) { return ((a % n) + n) % n; };
+    for (int k = 0; k < (int)sz; ++k)
+        for (int j = 0; j < (int)sy; ++j)
+            for (int i = 0; i < (int)sx; ++i) {
+                const int gi = (i < g || i >= g + nx), gj = (j < g || j >= g + ny),
+                          gk = (k < g || k >= g + nz);
+                if (gi + gj + gk > 1) continue;  // edge or corner ghost
+                const int ii = wrapi(i - g, nx), jj = wrapi(j - g, ny), kk = wrapi(k - g, nz);
+                dst[(k * sy + j) * sx + i] = src[((long long)kk * ny + jj) * nx + ii];
+            }
+}
+
+long long ghosted_count(const ns3d_params& p) {
+    const int g = p.ghost_layers;
+    return (long long)(p.global_nx + 2 * g) * (p.global_ny + 2 * g) * (p.global_nz + 2 * g);
+}
+
+// Upload 5 host arrays into 5 consecutive device arrays starting at dst.
+ns3d_status upload5(ns3d_ctx* ctx, const double* const* h, double* const* d, int layout) {
+    if (layout == NS3D_LAYOUT_INTERIOR) {
+        for (int q = 0; q < 5; ++q) {
+            if (!h[q]) return fail(ctx, NS3D_ERR_INVALID, "null host pointer");
+            NS3D_CK(cudaMemcpyAsync(d[q], h[q], sizeof(double) * ctx->n, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+        }
+        return NS3D_OK;
+    }
+    if (layout != NS3D_LAYOUT_GHOSTED) return fail(ctx, NS3D_ERR_INVALID, "unknown layout");
+    std::vector<double> tmp(ctx->n);
+    for (int q = 0; q < 5; ++q) {
+        if (!h[q]) return fail(ctx, NS3D_ERR_INVALID, "null host pointer");
+        gather_interior(ctx->p, h[q], tmp.data());
+        NS3D_CK(cudaMemcpyAsync(d[q], tmp.data(), sizeof(double) * ctx->n, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return NS3D_OK;
+}
+
+ns3d_status download_arrays(ns3d_ctx* ctx, const double* const* d, double* const* h,
+                            const double* fills, int count, int layout) {
+    if (layout == NS3D_LAYOUT_INTERIOR) {
+        for (int q = 0; q < count; ++q)
+            if (h[q])
+                NS3D_CK(cudaMemcpyAsync(h[q], d[q], sizeof(double) * ctx->n, cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+        return NS3D_OK;
+    }
+    if (layout != NS3D_LAYOUT_GHOSTED) return fail(ctx, NS3D_ERR_INVALID, "unknown layout");
+    std::vector<double> tmp(ctx->n);
+    for (int q = 0; q < count; ++q) {
+        if (!h[q]) continue;
+        NS3D_CK(cudaMemcpyAsync(tmp.data(), d[q], sizeof(double) * ctx->n, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+        scatter_ghosted(ctx->p, tmp.data(), h[q], fills[q]);
+    }
+    return NS3D_OK;
+}
+
+ns3d_status compute_sums(ns3d_ctx* ctx, double out[NSUMS]) {
+    NS3D_LAUNCH(NS3D_KERNEL_OTHER, 2, (k_sums_partial<<<ctx->sums_blocks, 256, 0, ctx->stream>>>(
+                                           ctx->L.P, view(ctx, ctx->cur), ctx->sums_part),
+                                       k_sums_final<<<1, 32, 0, ctx->stream>>>(
+                                           ctx->sums_part, ctx->sums_blocks, ctx->sums_out)));
+    NS3D_CK(cudaMemcpyAsync(out, ctx->sums_out, sizeof(double) * NSUMS, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char* ns3d_last_error(const ns3d_ctx* ctx) { return ctx ? ctx->err.c_str() : kStaticErr; }
+
+ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
+    if (!p || !out) return NS3D_ERR_INVALID;
+    *out = nullptr;
+    ns3d_params q = *p;
+    ns3d_status s = ns3d_params_derive(&q);
+    if (s != NS3D_OK) return s;
+    std::string msg;
+    s = validate(&q, msg);
+    if (s != NS3D_OK) {
+        std::fprintf(stderr, "ns3d_create: %s\n", msg.c_str());
+        return s;
+    }
+    auto* ctx = new ns3d_ctx;
+    ctx->p = q;
+    ctx->device = device;
+    ctx->n = (long long)q.global_nx * q.global_ny * q.global_nz;
+    ctx->time = 0.0;
+    ctx->out_next = q.output_Timefreq;
+    DevParams& P = ctx->L.P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = q.global_nx; P.ny = q.global_ny; P.nz = q.global_nz; P.n = ctx->n;
+    P.gamma = q.gamma; P.Rgas = q.Rgas; P.mu = q.mu; P.Cp = q.Cp; P.Pr = q.Pr;
+    P.sutherland_s = q.sutherland_s_over_tref; P.sw_eps = q.sw_entropy_eps;
+    P.dx = q.dx; P.dy = q.dy; P.dz = q.dz;
+    P.inv_dx = 1.0 / q.dx; P.inv_dy = 1.0 / q.dy; P.inv_dz = 1.0 / q.dz;  // range_kutta.cpp:14-16
+    P.cfl = q.cfl; P.dt_fixed = q.dt_fixed;
+    linear_coefficients(q, P.lin);
+    P.mdcd_disp = q.mdcd_disp; P.mdcd_diss = q.mdcd_diss;
+    P.vis_order = q.vis_scheme == NS3D_VIS_C4TH ? 4 : (q.vis_scheme == NS3D_VIS_C6TH ? 6 : 8);
+    ctx->L.fvs = q.fvs_type == NS3D_FVS_STEGER_WARMING ? FV_SW : FV_LF;
+    ctx->L.rc = recon_kind(q.recon);
+    for (int d = 0; d < 3; ++d) ctx->L.seg[d] = 32;
+    ctx->rsize = q.precision == NS3D_PREC_FP64 ? sizeof(double) : sizeof(float);
+
+    auto bail = [&](ns3d_status st, const std::string& m) {
+        std::fprintf(stderr, "ns3d_create: %s\n", m.c_str());
+        ns3d_destroy(ctx);
+        return st;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bail(NS3D_ERR_CUDA, cudaGetErrorString(e));
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(NS3D_ERR_CUDA, cudaGetErrorString(e));
+    ctx->L.stream = ctx->stream;
+    const size_t n = (size_t)ctx->n;
+    if (cudaMalloc(&ctx->wmem, sizeof(double) * 18 * n) != cudaSuccess ||
+        cudaMalloc(&ctx->tacc, ctx->rsize * 5 * n) != cudaSuccess ||
+        cudaMalloc(&ctx->fv, ctx->rsize * 9 * n) != cudaSuccess ||
+        cudaMalloc(&ctx->ctrl, sizeof(Ctrl)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(NS3D_ERR_NOMEM, "device allocation failed");
+    }
+    if (cudaMallocHost(&ctx->ctrl_host, sizeof(Ctrl)) != cudaSuccess)
+        return bail(NS3D_ERR_NOMEM, "pinned allocation failed");
+    ctx->sums_blocks = (int)std::min<long long>(4 * 148, (ctx->n + 255) / 256);
+    if (cudaMalloc(&ctx->sums_part, sizeof(double) * NSUMS * ctx->sums_blocks) != cudaSuccess ||
+        cudaMalloc(&ctx->sums_out, sizeof(double) * NSUMS) != cudaSuccess)
+        return bail(NS3D_ERR_NOMEM, "device allocation failed");
+    // a uniform quiescent state until the first upload (Field3D::allocate, :232-236)
+    cudaMemsetAsync(ctx->wmem, 0, sizeof(double) * 18 * n, ctx->stream);
+    if (reset_ctrl(ctx) != NS3D_OK) return bail(NS3D_ERR_CUDA, ctx->err);
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+        return bail(NS3D_ERR_CUDA, cudaGetErrorString(e));
+    *out = ctx;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->fft_ready) cufftDestroy(ctx->fft);
+    cudaFree(ctx->spec);
+    cudaFree(ctx->bins);
+    cudaFree(ctx->wmem);
+    cudaFree(ctx->tacc);
+    cudaFree(ctx->fv);
+    cudaFree(ctx->ctrl);
+    cudaFree(ctx->sums_part);
+    cudaFree(ctx->sums_out);
+    if (ctx->ctrl_host) cudaFreeHost(ctx->ctrl_host);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_get_params(const ns3d_ctx* ctx, ns3d_params* out) {
+    if (!ctx || !out) return NS3D_ERR_INVALID;
+    *out = ctx->p;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_device_bytes(const ns3d_ctx* ctx, size_t* bytes) {
+    if (!ctx || !bytes) return NS3D_ERR_INVALID;
+    *bytes = sizeof(double) * 18 * (size_t)ctx->n + ctx->rsize * 14 * (size_t)ctx->n;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_synchronize(ns3d_ctx* ctx) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_upload_primitive(ns3d_ctx* ctx, const double* rho, const double* u,
+                                  const double* v, const double* w, const double* p, int layout) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const double* h[5] = {rho, u, v, w, p};
+    double* d[5];
+    for (int q = 0; q < 5; ++q) d[q] = warr(ctx, ctx->cur, q);
+    ns3d_status s = upload5(ctx, h, d, layout);
+    if (s != NS3D_OK) return s;
+    k_prim_finish<<<blocks_for(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->L.P, outv(ctx, ctx->cur));
+    NS3D_CK(cudaGetLastError());
+    ctx->rec = ctx->cur;
+    ctx->dtmin_valid = false;
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_upload_conserved(ns3d_ctx* ctx, const double* rho, const double* rhou,
+                                  const double* rhov, const double* rhow, const double* E,
+                                  int layout) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const int tmpb = (ctx->cur + 1) % 3;  // a free state buffer as staging (5 of its 6 arrays)
+    const double* h[5] = {rho, rhou, rhov, rhow, E};
+    double* d[5];
+    for (int q = 0; q < 5; ++q) d[q] = warr(ctx, tmpb, q);
+    ns3d_status s = upload5(ctx, h, d, layout);
+    if (s != NS3D_OK) return s;
+    k_cons2prim<<<blocks_for(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->L.P, warr(ctx, tmpb, 0),
+                                                                 outv(ctx, ctx->cur));
+    NS3D_CK(cudaGetLastError());
+    ctx->rec = ctx->cur;
+    ctx->dtmin_valid = false;
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_download_primitive(ns3d_ctx* ctx, double* rho, double* u, double* v, double* w,
+                                    double* p, double* T, double* c, int layout) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const double* d[7];
+    for (int q = 0; q < 6; ++q) d[q] = warr(ctx, ctx->cur, q);
+    d[6] = nullptr;
+    if (c) {
+        // c from primitiveToConserved; staged in a free buffer
+        const int tmpb = ctx->cur == ctx->rec ? (ctx->cur + 1) % 3 : 3 - ctx->cur - ctx->rec;
+        k_prim2cons<<<blocks_for(ctx->n, 256), 256, 0, ctx->stream>>>(
+            ctx->L.P, view(ctx, ctx->cur), warr(ctx, tmpb, 0), warr(ctx, tmpb, 5));
+        NS3D_CK(cudaGetLastError());
+        d[6] = warr(ctx, tmpb, 5);
+    }
+    double* h[7] = {rho, u, v, w, p, T, c};
+    const double fills[7] = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    return download_arrays(ctx, d, h, fills, 7, layout);
+}
+
+ns3d_status ns3d_download_conserved(ns3d_ctx* ctx, double* rho, double* rhou, double* rhov,
+                                    double* rhow, double* E, int layout) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const int tmpb = ctx->cur == ctx->rec ? (ctx->cur + 1) % 3 : 3 - ctx->cur - ctx->rec;
+    k_prim2cons<<<blocks_for(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->L.P, view(ctx, ctx->cur),
+                                                                 warr(ctx, tmpb, 0), nullptr);
+    NS3D_CK(cudaGetLastError());
+    const double* d[5];
+    for (int q = 0; q < 5; ++q) d[q] = warr(ctx, tmpb, 0) + q * ctx->n;
+    double* h[5] = {rho, rhou, rhov, rhow, E};
+    const double fills[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
+    return download_arrays(ctx, d, h, fills, 5, layout);
+}
+
+ns3d_status ns3d_record_conserved0(ns3d_ctx* ctx) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    ctx->rec = ctx->cur;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_compute_rhs(ns3d_ctx* ctx, double* r0, double* r1, double* r2, double* r3,
+                             double* r4, int layout) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    ns3d_status s = launch_rhs_parts(ctx, view(ctx, ctx->cur), nullptr);
+    if (s != NS3D_OK) return s;
+    // rhs staged in a free state buffer (5 of its 6 arrays)
+    const int tmpb = ctx->cur == ctx->rec ? (ctx->cur + 1) % 3 : 3 - ctx->cur - ctx->rec;
+    double* rhs = warr(ctx, tmpb, 0);
+    if (ctx->p.precision == NS3D_PREC_FP64)
+        NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                    launch_rhs_out<double>(ctx->L, (const double*)ctx->tacc, (const double*)ctx->fv, rhs));
+    else
+        NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                    launch_rhs_out<float>(ctx->L, (const float*)ctx->tacc, (const float*)ctx->fv, rhs));
+    const double* d[5];
+    for (int q = 0; q < 5; ++q) d[q] = rhs + q * ctx->n;
+    double* h[5] = {r0, r1, r2, r3, r4};
+    const double fills[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    return download_arrays(ctx, d, h, fills, 5, layout);
+}
+
+ns3d_status ns3d_compute_timestep(ns3d_ctx* ctx, double* dt) {
+    if (!ctx || !dt) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    ns3d_status s = reset_ctrl(ctx);
+    if (s != NS3D_OK) return s;
+    if ((s = enqueue_cfl(ctx)) != NS3D_OK) return s;
+    if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
+    double m;
+    std::memcpy(&m, &ctx->ctrl_host->dtmin_bits, sizeof(double));
+    *dt = ctx->p.cfl * m;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_runge_kutta_3(ns3d_ctx* ctx, double dt) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    ns3d_status s = reset_ctrl(ctx);
+    if (s != NS3D_OK) return s;
+    NS3D_CK(cudaMemcpyAsync(&ctx->ctrl->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = enqueue_rk3(ctx)) != NS3D_OK) return s;
+    ctx->dtmin_valid = true;  // stage 3 left the CFL minimum of the new state in ctrl
+    if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
+    if (ctx->ctrl_host->bad_cell < ctx->n) {
+        char buf[160];
+        const long long b = ctx->ctrl_host->bad_cell;
+        std::snprintf(buf, sizeof(buf), "non-physical value at cell (%lld,%lld,%lld)",
+                      b % ctx->p.global_nx, (b / ctx->p.global_nx) % ctx->p.global_ny,
+                      b / ((long long)ctx->p.global_nx * ctx->p.global_ny));
+        return fail(ctx, NS3D_ERR_NONPHYSICAL, buf);
+    }
+    return NS3D_OK;
+}
+
+static ns3d_status run_steps(ns3d_ctx* ctx, int mode, int nsteps, int* steps_done) {
+    NS3D_CK(cudaSetDevice(ctx->device));
+    // keep the CFL minimum of the current state across calls when valid
+    unsigned long long keep = 0;
+    bool have = false;
+    if (ctx->dtmin_valid) {
+        NS3D_CK(cudaMemcpyAsync(&keep, &ctx->ctrl->dtmin_bits, sizeof(keep), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+        have = true;
+    }
+    ns3d_status s = reset_ctrl(ctx);
+    if (s != NS3D_OK) return s;
+    if (have)
+        NS3D_CK(cudaMemcpyAsync(&ctx->ctrl->dtmin_bits, &keep, sizeof(keep), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    else if ((s = enqueue_cfl(ctx)) != NS3D_OK)
+        return s;
+    const ns3d_params& p = ctx->p;
+    const int cur0 = ctx->cur, rec0 = ctx->rec;
+    for (int step = 0; step < nsteps; ++step) {
+        ctx->rec = ctx->cur;  // recordConservedTo0 (maincycle.cpp:22)
+        NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                    (k_control_pre<<<1, 1, 0, ctx->stream>>>(ctx->ctrl, mode, p.cfl, p.dt_fixed,
+                                                              p.TotalTime, p.output_Timefreq)));
+        if ((s = enqueue_rk3(ctx)) != NS3D_OK) return s;
+        NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                    (k_control_post<<<1, 1, 0, ctx->stream>>>(ctx->ctrl, mode, p.TotalTime, ctx->n)));
+    }
+    if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
+    const Ctrl& h = *ctx->ctrl_host;
+    // Kernels of the iterations after a device-side stop returned at entry, so
+    // the buffer rotation is that of the completed steps only: each step with
+    // U0 recorded from the current buffer moves `cur` one buffer forward.
+    const int d = h.steps_done;
+    ctx->cur = (cur0 + d) % 3;
+    if (nsteps == 0) ctx->rec = rec0;
+    else if (d < nsteps && h.stop_in_pre) ctx->rec = ctx->cur;  // recorded, then stopped
+    else ctx->rec = d > 0 ? (cur0 + d - 1) % 3 : rec0;
+    if (steps_done) *steps_done = d;
+    ctx->time = h.time;
+    ctx->out_next = h.out_next;
+    ctx->dtmin_valid = true;
+    if (h.stop && h.stop_reason == STOP_NONPHYSICAL) return fail(ctx, NS3D_ERR_NONPHYSICAL, "non-physical state");
+    if (h.stop && h.stop_reason == STOP_DT_SMALL) return fail(ctx, NS3D_ERR_DT, "dt too small");
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_step(ns3d_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return NS3D_ERR_INVALID;
+    return run_steps(ctx, 0, nsteps, nullptr);
+}
+
+ns3d_status ns3d_time_advance(ns3d_ctx* ctx, int max_steps, double* time, int* steps_done) {
+    if (!ctx || max_steps < 0) return NS3D_ERR_INVALID;
+    int done = 0;
+    ns3d_status s = run_steps(ctx, 1, max_steps, &done);
+    if (time) *time = ctx->time;
+    if (steps_done) *steps_done = done;
+    return s;
+}
+
+ns3d_status ns3d_last_dt(ns3d_ctx* ctx, double* dt) {
+    if (!ctx || !dt) return NS3D_ERR_INVALID;
+    ns3d_status s = read_ctrl(ctx);
+    if (s != NS3D_OK) return s;
+    *dt = ctx->ctrl_host->dt;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_total_energy(ns3d_ctx* ctx, double* etot) {
+    if (!ctx || !etot) return NS3D_ERR_INVALID;
+    double s[NSUMS];
+    ns3d_status st = compute_sums(ctx, s);
+    if (st != NS3D_OK) return st;
+    *etot = s[0] * (ctx->p.dx * ctx->p.dy * ctx->p.dz);
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_energy_spectrum(ns3d_ctx* ctx, double* Ek, int nbins) {
+    if (!ctx || !Ek || nbins <= 0 || nbins > 2 * ctx->p.global_nx + 1) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const int nx = ctx->p.global_nx, ny = ctx->p.global_ny, nz = ctx->p.global_nz;
+    const int kmax = 2 * nx + 1;
+    if (!ctx->fft_ready) {
+        if (cufftPlan3d(&ctx->fft, nz, ny, nx, CUFFT_D2Z) != CUFFT_SUCCESS)
+            return fail(ctx, NS3D_ERR_CUDA, "cufftPlan3d failed");
+        cufftSetStream(ctx->fft, ctx->stream);
+        NS3D_CK(cudaMalloc(&ctx->spec, sizeof(cufftDoubleComplex) * (size_t)(nx / 2 + 1) * ny * nz));
+        NS3D_CK(cudaMalloc(&ctx->bins, sizeof(double) * kmax));
+        ctx->fft_ready = true;
+    }
+    NS3D_CK(cudaMemsetAsync(ctx->bins, 0, sizeof(double) * kmax, ctx->stream));
+    const double scale = 1.0 / (double)ctx->n;  // EnergySpectrum.cpp:88-96
+    for (int comp = 1; comp <= 3; ++comp) {
+        if (cufftExecD2Z(ctx->fft, warr(ctx, ctx->cur, comp), ctx->spec) != CUFFT_SUCCESS)
+            return fail(ctx, NS3D_ERR_CUDA, "cufftExecD2Z failed");
+        k_spectrum_bin<<<4 * 148, 256, sizeof(double) * kmax, ctx->stream>>>(ctx->spec, nx, ny, nz,
+                                                                             scale, kmax, ctx->bins);
+        NS3D_CK(cudaGetLastError());
+    }
+    NS3D_CK(cudaMemcpyAsync(Ek, ctx->bins, sizeof(double) * nbins, cudaMemcpyDeviceToHost, ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_get_stream(ns3d_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return NS3D_ERR_INVALID;
+    *stream = (void*)ctx->stream;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_profile(ns3d_ctx* ctx, int enable) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    if (enable) {
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+        ctx->prof.clear();
+        ctx->ev_used = 0;
+    }
+    ctx->prof_on = enable != 0;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_profile_read(ns3d_ctx* ctx, double* ms, long long* launches) {
+    if (!ctx || !ms || !launches) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    for (int c = 0; c < NS3D_KERNEL_CLASSES; ++c) {
+        ms[c] = 0.0;
+        launches[c] = 0;
+    }
+    for (const auto& r : ctx->prof) {
+        float t = 0.f;
+        NS3D_CK(cudaEventElapsedTime(&t, r.a, r.b));
+        ms[r.cls] += t;
+        launches[r.cls] += 1;
+    }
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_launch_count(const ns3d_ctx* ctx, long long* count) {
+    if (!ctx || !count) return NS3D_ERR_INVALID;
+    *count = ctx->launches;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_turbulence_stats(ns3d_ctx* ctx, ns3d_turb_stats* out) {
+    if (!ctx || !out) return NS3D_ERR_INVALID;
+    double s[NSUMS];
+    ns3d_status st = compute_sums(ctx, s);
+    if (st != NS3D_OK) return st;
+    const int kmax = 2 * ctx->p.global_nx + 1;
+    std::vector<double> Ek(kmax);
+    if ((st = ns3d_energy_spectrum(ctx, Ek.data(), kmax)) != NS3D_OK) return st;
+    const double N = (double)ctx->n;
+    std::memset(out, 0, sizeof(*out));
+    out->total_energy = s[0] * (ctx->p.dx * ctx->p.dy * ctx->p.dz);
+    out->mean_mu = s[2] / N;
+    out->mean_rho = s[3] / N;
+    out->nu = out->mean_mu / out->mean_rho;
+    out->kinetic_energy = s[1] / N;
+    out->u_rms = std::sqrt(s[4] / (3.0 * N));
+    const double mu_ = s[5] / N, mv = s[6] / N, mw = s[7] / N;
+    out->tke = 0.5 * ((s[8] / N - mu_ * mu_) + (s[9] / N - mv * mv) + (s[10] / N - mw * mw));
+    out->mach_t = std::sqrt(out->kinetic_energy * 2) / (s[11] / N);
+    double eps = 0.0;
+    for (int k = 0; k < kmax; ++k) eps += 2.0 * out->nu * (double)k * (double)k * Ek[k];
+    out->dissipation = eps;
+    return NS3D_OK;
+}
+
+}  // extern "C"

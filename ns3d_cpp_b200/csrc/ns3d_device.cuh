@@ -1,0 +1,244 @@
+// Per-cell device functions of the RHS: thermodynamics, flux vector splitting,
+// scalar reconstructions, central differences.
+//
+// Templated on the compute type R. The FP64 instantiation is compiled with
+// -fmad=false and keeps the reference's expression order term by term, so it
+// reproduces the reference's rounding (IEEE division and sqrt are correctly
+// rounded on both sides; pow may differ by an ulp). The FP32 instantiation
+// runs the same algebra in float (the FP32-stencil form).
+#pragma once
+
+#include <cstdint>
+
+namespace ns3d {
+
+// Scheme identifiers used as template arguments. Linear schemes share one
+// code path: MDCD (reconstruction.cpp:126-135) is a 6-point linear stencil and
+// UPWIND_7TH / UD7L (:227-249) are 8-point linear stencils whose coefficients
+// are evaluated on the host with the reference's expressions.
+enum : int { RC_WENO5 = 0, RC_LINEAR = 2, RC_LIN6 = 3, RC_MDCD_HYBRID = 4, RC_LIN8 = 5 };
+enum : int { FV_SW = 0, FV_LF = 1 };
+
+template <int RC> struct Stencil;
+template <> struct Stencil<RC_WENO5> { static constexpr int S = 6; };
+template <> struct Stencil<RC_LINEAR> { static constexpr int S = 2; };
+template <> struct Stencil<RC_LIN6> { static constexpr int S = 6; };
+template <> struct Stencil<RC_MDCD_HYBRID> { static constexpr int S = 6; };
+template <> struct Stencil<RC_LIN8> { static constexpr int S = 8; };
+
+// Parameters every kernel receives by value.
+struct DevParams {
+    int nx, ny, nz;
+    long long n;
+    double gamma, Rgas, mu, Cp, Pr, sutherland_s, sw_eps;
+    double dx, dy, dz, inv_dx, inv_dy, inv_dz;
+    double cfl, dt_fixed;
+    double lin[8];   // linear reconstruction coefficients (LIN6 / LIN8)
+    double mdcd_disp, mdcd_diss;
+    int vis_order;   // 4, 6, 8
+};
+
+// ---------------------------------------------------------------------------
+// Thermodynamics (field_structures.h:94-105, 405-451)
+// ---------------------------------------------------------------------------
+
+// SolverParams::get_mu (field_structures.h:94-105): Sutherland.
+template <class R>
+__device__ __forceinline__ R get_mu(R T, R mu_ref, R S) {
+    return mu_ref * pow(T, R(1.5)) * (R(1.0) + S) / (T + S);
+}
+
+// primitiveToConserved (field_structures.h:430-451) for one cell: E and c.
+template <class R>
+__device__ __forceinline__ void p2c_Ec(R rr, R u, R v, R w, R p, R gamma, R& E, R& c) {
+    R kinetic = R(0.5) * (u * u + v * v + w * w);
+    R e_internal = p / ((gamma - R(1.0)) * rr);
+    E = rr * (e_internal + kinetic);
+    c = sqrt(gamma * p / rr);
+}
+
+// ---------------------------------------------------------------------------
+// Flux vector splitting (InviscousFlux_new.cpp:439-530)
+// ---------------------------------------------------------------------------
+
+template <class R>
+__device__ __forceinline__ R abs_fix(R l, R eps) {
+    // README.md:177-180 entropy fix; eps == 0 is the reference's plain |l|.
+    return eps > R(0) ? sqrt(l * l + eps * eps) : fabs(l);
+}
+
+// split_StagerWarming (InviscousFlux_new.cpp:439-489). N1,N2,N3: direction.
+template <class R, int N1, int N2, int N3>
+__device__ __forceinline__ void split_sw(R rho, R u, R v, R w, R E, R p, R c, R gamma, R eps,
+                                         R Fp[5], R Fm[5]) {
+    const R n1 = R(N1), n2 = R(N2), n3 = R(N3);
+    R un = u * n1 + v * n2 + w * n3;
+    R lambda1 = un - c, lambda2 = un, lambda3 = un + c;
+    R a1 = abs_fix(lambda1, eps), a2 = abs_fix(lambda2, eps), a3 = abs_fix(lambda3, eps);
+    R lambda1_plus = R(0.5) * (lambda1 + a1);
+    R lambda1_minus = R(0.5) * (lambda1 - a1);
+    R lambda2_plus = R(0.5) * (lambda2 + a2);
+    R lambda2_minus = R(0.5) * (lambda2 - a2);
+    R lambda3_plus = R(0.5) * (lambda3 + a3);
+    R lambda3_minus = R(0.5) * (lambda3 - a3);
+    R S1_p = lambda1_plus + lambda3_plus;
+    R S1_m = lambda1_minus + lambda3_minus;
+    R S2_p = lambda3_plus - lambda1_plus;
+    R S2_m = lambda3_minus - lambda1_minus;
+    R H = (E + p) / rho;
+    R ga1 = rho / (R(2.0) * gamma);
+    R ga2 = R(2.0) * (gamma - R(1.0));
+    R V = R(0.5) * (u * u + v * v + w * w);
+    Fp[0] = ga1 * (S1_p + ga2 * lambda2_plus);
+    Fp[1] = ga1 * (S1_p * u + ga2 * lambda2_plus * u + S2_p * n1 * c);
+    Fp[2] = ga1 * (S1_p * v + ga2 * lambda2_plus * v + S2_p * n2 * c);
+    Fp[3] = ga1 * (S1_p * w + ga2 * lambda2_plus * w + S2_p * n3 * c);
+    Fp[4] = ga1 * (S1_p * H + ga2 * lambda2_plus * V + S2_p * un * c);
+    Fm[0] = ga1 * (S1_m + ga2 * lambda2_minus);
+    Fm[1] = ga1 * (S1_m * u + ga2 * lambda2_minus * u + S2_m * n1 * c);
+    Fm[2] = ga1 * (S1_m * v + ga2 * lambda2_minus * v + S2_m * n2 * c);
+    Fm[3] = ga1 * (S1_m * w + ga2 * lambda2_minus * w + S2_m * n3 * c);
+    Fm[4] = ga1 * (S1_m * H + ga2 * lambda2_minus * V + S2_m * un * c);
+}
+
+// split_LaxFriedrichs (InviscousFlux_new.cpp:491-530), local wave speed.
+template <class R, int N1, int N2, int N3>
+__device__ __forceinline__ void split_lf(R rho, R u, R v, R w, R E, R p, R c, R Fp[5],
+                                         R Fm[5]) {
+    const R n1 = R(N1), n2 = R(N2), n3 = R(N3);
+    R un = u * n1 + v * n2 + w * n3;
+    R a_max = fabs(un) + c;
+    R F1 = rho * un;
+    R F2 = rho * u * un + p * n1;
+    R F3 = rho * v * un + p * n2;
+    R F4 = rho * w * un + p * n3;
+    R F5 = (E + p) * un;
+    Fp[0] = R(0.5) * (F1 + a_max * rho);
+    Fp[1] = R(0.5) * (F2 + a_max * rho * u);
+    Fp[2] = R(0.5) * (F3 + a_max * rho * v);
+    Fp[3] = R(0.5) * (F4 + a_max * rho * w);
+    Fp[4] = R(0.5) * (F5 + a_max * E);
+    Fm[0] = R(0.5) * (F1 - a_max * rho);
+    Fm[1] = R(0.5) * (F2 - a_max * rho * u);
+    Fm[2] = R(0.5) * (F3 - a_max * rho * v);
+    Fm[3] = R(0.5) * (F4 - a_max * rho * w);
+    Fm[4] = R(0.5) * (F5 - a_max * E);
+}
+
+// ---------------------------------------------------------------------------
+// Scalar reconstructions (reconstruction.cpp). `s` is the window after the
+// reversal that reconstruct_select applies for the minus flux (:24-31).
+// ---------------------------------------------------------------------------
+
+// weno5_reconstruction (reconstruction.cpp:93-124): WENO5-JS, eps 1e-6, p = 2.
+template <class R>
+__device__ __forceinline__ R weno5(R f0, R f1, R f2, R f3, R f4) {
+    const R eps = R(1e-6);
+    R beta0 = R(13.0 / 12.0) * (f0 - R(2) * f1 + f2) * (f0 - R(2) * f1 + f2)
+            + R(0.25) * (f0 - R(4) * f1 + R(3) * f2) * (f0 - R(4) * f1 + R(3) * f2);
+    R beta1 = R(13.0 / 12.0) * (f1 - R(2) * f2 + f3) * (f1 - R(2) * f2 + f3)
+            + R(0.25) * (f1 - f3) * (f1 - f3);
+    R beta2 = R(13.0 / 12.0) * (f2 - R(2) * f3 + f4) * (f2 - R(2) * f3 + f4)
+            + R(0.25) * (R(3) * f2 - R(4) * f3 + f4) * (R(3) * f2 - R(4) * f3 + f4);
+    R alpha0 = R(0.1) / ((eps + beta0) * (eps + beta0));
+    R alpha1 = R(0.6) / ((eps + beta1) * (eps + beta1));
+    R alpha2 = R(0.3) / ((eps + beta2) * (eps + beta2));
+    R asum = alpha0 + alpha1 + alpha2;
+    R w0 = alpha0 / asum;
+    R w1 = alpha1 / asum;
+    R w2 = alpha2 / asum;
+    R p0 = (R(2) * f0 - R(7) * f1 + R(11) * f2) / R(6.0);
+    R p1 = (-f1 + R(5) * f2 + R(2) * f3) / R(6.0);
+    R p2 = (R(2) * f2 + R(5) * f3 - f4) / R(6.0);
+    return w0 * p0 + w1 * p1 + w2 * p2;
+}
+
+// mdcd_hybrid_reconstruction (reconstruction.cpp:151-225).
+template <class R>
+__device__ __forceinline__ R mdcd_hybrid(const R* s, const R* lin6, R disp, R diss) {
+    const R eps_small = R(1e-40);
+    R f0 = s[0], f1 = s[1], f2 = s[2], f3 = s[3], f4 = s[4], f5 = s[5];
+    const R eps = R(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
+    R a1 = fabs(f2 - f1) + fabs(f2 - R(2) * f1 + f0);
+    R b1 = fabs(f2 - f3) + fabs(f2 - R(2) * f3 + f4);
+    R a2 = fabs(f3 - f2) + fabs(f3 - R(2) * f2 + f1);
+    R b2 = fabs(f3 - f4) + fabs(f3 - R(2) * f4 + f5);
+    R sai1 = (R(2) * a1 * b1 + eps) / (a1 * a1 + b1 * b1 + eps);
+    R sai2 = (R(2) * a2 * b2 + eps) / (a2 * a2 + b2 * b2 + eps);
+    R sai = sai2 < sai1 ? sai2 : sai1;
+    if (sai > R(0.4)) {
+        return lin6[0] * s[0] + lin6[1] * s[1] + lin6[2] * s[2] + lin6[3] * s[3] +
+               lin6[4] * s[4] + lin6[5] * s[5];
+    }
+    R q0 = (R(2) * f0 - R(7) * f1 + R(11) * f2) / R(6.0);
+    R q1 = (-f1 + R(5) * f2 + R(2) * f3) / R(6.0);
+    R q2 = (R(2) * f2 + R(5) * f3 - f4) / R(6.0);
+    R q3 = (R(11) * f3 - R(7) * f4 + R(2) * f5) / R(6.0);
+    R d0 = R(1.5) * (disp + diss);
+    R d1 = R(0.5) - R(1.5) * (disp - R(3) * diss);
+    R d2 = R(0.5) - R(1.5) * (disp + R(3) * diss);
+    R d3 = R(1.5) * (disp - diss);
+    R t;
+    t = f0 - R(2) * f1 + f2; R e0 = t * t; t = f0 - R(4) * f1 + R(3) * f2; R g0 = t * t;
+    R beta0 = R(13.0 / 12.0) * e0 + R(0.25) * g0;
+    t = f1 - R(2) * f2 + f3; R e1 = t * t; t = f1 - f3; R g1 = t * t;
+    R beta1 = R(13.0 / 12.0) * e1 + R(0.25) * g1;
+    t = f2 - R(2) * f3 + f4; R e2 = t * t; t = R(3) * f2 - R(4) * f3 + f4; R g2 = t * t;
+    R beta2 = R(13.0 / 12.0) * e2 + R(0.25) * g2;
+    R beta3 = (R(271799) * (f0 * f0)
+        + f0 * (R(-2380800) * f1 + R(4086352) * f2 - R(3462252) * f3 + R(1458762) * f4 - R(245620) * f5)
+        + f1 * (R(5653317) * f1 - R(20427884) * f2 + R(17905032) * f3 - R(7727988) * f4 + R(1325006) * f5)
+        + f2 * (R(19510972) * f2 - R(35817664) * f3 + R(15929912) * f4 - R(2792660) * f5)
+        + f3 * (R(17195652) * f3 - R(15880404) * f4 + R(2863984) * f5)
+        + f4 * (R(3824847) * f4 - R(1429976) * f5)
+        + R(139633) * (f5 * f5)) / R(120960.0);
+    R tau6 = fabs(beta3 - (beta0 + R(4) * beta1 + beta2) / R(6.0));
+    t = R(20) + tau6 / (beta0 + eps_small); R aa0 = d0 * (t * t);
+    t = R(20) + tau6 / (beta1 + eps_small); R aa1 = d1 * (t * t);
+    t = R(20) + tau6 / (beta2 + eps_small); R aa2 = d2 * (t * t);
+    t = R(20) + tau6 / (beta3 + eps_small); R aa3 = d3 * (t * t);
+    return (aa0 * q0 + aa1 * q1 + aa2 * q2 + aa3 * q3) / (aa0 + aa1 + aa2 + aa3);
+}
+
+// One reconstruction of a window s[0..S-1] (already oriented).
+template <class R, int RC>
+__device__ __forceinline__ R reconstruct(const R* s, const R* lin, R disp, R diss) {
+    if constexpr (RC == RC_WENO5) {
+        return weno5(s[0], s[1], s[2], s[3], s[4]);
+    } else if constexpr (RC == RC_LINEAR) {
+        return s[0];  // linear_reconstruction, reconstruction.cpp:88-90
+    } else if constexpr (RC == RC_LIN6) {
+        return lin[0] * s[0] + lin[1] * s[1] + lin[2] * s[2] + lin[3] * s[3] + lin[4] * s[4] +
+               lin[5] * s[5];
+    } else if constexpr (RC == RC_MDCD_HYBRID) {
+        return mdcd_hybrid(s, lin, disp, diss);
+    } else {
+        return lin[0] * s[0] + lin[1] * s[1] + lin[2] * s[2] + lin[3] * s[3] + lin[4] * s[4] +
+               lin[5] * s[5] + lin[6] * s[6] + lin[7] * s[7];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Central first derivatives (ViscousFlux.cpp:23-40); periodic => full order.
+// f(o) returns the value at offset o along the line.
+// ---------------------------------------------------------------------------
+template <class R, int ORD, class F>
+__device__ __forceinline__ R dcentral(F f, R h) {
+    if constexpr (ORD == 4) {
+        return (-f(2) + R(8.0) * f(1) - R(8.0) * f(-1) + f(-2)) / (R(12.0) * h);
+    } else if constexpr (ORD == 6) {
+        return (f(3) - R(9.0) * f(2) + R(45.0) * f(1) - R(45.0) * f(-1) + R(9.0) * f(-2) - f(-3)) /
+               (R(60.0) * h);
+    } else {
+        const R c1 = R(0.8), c2 = R(-0.2), c3 = R(0.0380952380952381), c4 = R(-0.00357142857142857);
+        return (c1 * (f(1) - f(-1)) + c2 * (f(2) - f(-2)) + c3 * (f(3) - f(-3)) +
+                c4 * (f(4) - f(-4))) / h;
+    }
+}
+
+// Order-preserving bit pattern of a non-negative double (for atomicMin).
+__device__ __forceinline__ unsigned long long pos_double_bits(double x) {
+    return (unsigned long long)__double_as_longlong(x);
+}
+
+}  // namespace ns3d

@@ -1,0 +1,517 @@
+// Kernels of one RK3 stage, templated on the compute type R (double or float).
+//
+// Device layout (HBM): interior-only SoA arrays of n = nx*ny*nz doubles,
+// x fastest. The periodic ghost fill of the reference (apply_boundary +
+// primitiveToConserved, field_structures.h:795-853) becomes index wrap-around
+// in the loaders: a ghost value of the reference is bit-identical to its
+// periodic image, so nothing is copied.
+//
+// State per buffer: primitives rho,u,v,w,p plus T (= p/(rho Rgas) exactly as
+// primitiveToConserved computes it). Conserved values (rhou, E) and c are
+// recomputed on the fly with the reference's expressions, which reproduces
+// the cons->prim->cons round trip of every stage bit for bit.
+//
+// One stage = sweep_x, sweep_y, sweep_z (inviscid, accumulating
+// T_acc = ((ax*idx + ay*idy) + az*idz) in the reference's order), visc_flux
+// (gradients + stresses), update (viscous divergence, rhs, Shu-Osher stage in
+// double, conservedToPrimitive, next-step CFL candidates and positivity after
+// stage 3).
+#pragma once
+
+#include "ns3d_device.cuh"
+
+namespace ns3d {
+
+struct StateView {
+    const double *rho, *u, *v, *w, *p, *T;
+};
+struct StateOut {
+    double *rho, *u, *v, *w, *p, *T;
+};
+
+// Device-side control block of the time loop (maincycle.cpp:14-52).
+struct Ctrl {
+    unsigned long long dtmin_bits;   // running min of the CFL candidates (bit pattern)
+    unsigned long long pad0;
+    double dt;                       // dt of the step in flight
+    double time;                     // current_time
+    double out_next;                 // next scheduled output time
+    int stop;                        // 1: the loop has ended, kernels return at entry
+    int stop_reason;                 // NS3D_STOP_*
+    int steps_done;
+    int active;                      // a step is in flight
+    long long bad_cell;              // first non-physical cell (linear index), or n
+    int stop_in_pre;                 // the stop came from the start-of-iteration checks
+    int pad1;
+};
+
+enum : int { STOP_NONE = 0, STOP_TOTAL_TIME = 1, STOP_DT_SMALL = 2, STOP_NONPHYSICAL = 3 };
+
+constexpr double CFL_INIT = 1e9;     // timestep.cpp:8
+
+__device__ __forceinline__ int wrap1(int s, int len) {
+    return s < 0 ? s + len : (s >= len ? s - len : s);
+}
+
+// ---------------------------------------------------------------------------
+// Inviscid sweep along DIR (du_inviscous, InviscousFlux_new.cpp:4-163, and the
+// divergence of range_kutta.cpp:51-98).
+//
+// One thread marches along one line segment of `seg` cells, holding the split
+// fluxes of the S cells of the current face window in registers: each cell is
+// split once, every face is reconstructed once, and the face flux of the
+// previous face is kept for the difference. Split fluxes never touch memory.
+//   DIR 0: lines over (j,k), threads over j        (march along x)
+//   DIR 1: lines over (i,k), threads over i        (coalesced along x)
+//   DIR 2: lines over (i,j), threads over i        (coalesced along x)
+// T_acc (5 blocks of n, type R): DIR 0 writes ax*idx, DIR 1 and 2 add.
+// ---------------------------------------------------------------------------
+template <int DIR, class R, int FVS, int RC>
+__global__ void __launch_bounds__(128)
+k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __restrict__ ctrl) {
+    if (ctrl && ctrl->stop) return;
+    constexpr int S = Stencil<RC>::S;
+    constexpr int MID = (S - 1) / 2;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = P.n;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    long long base, stride;
+    int len;
+    if constexpr (DIR == 0) {
+        if (t0 >= ny) return;
+        base = ((long long)blockIdx.y * ny + t0) * nx;
+        stride = 1;
+        len = nx;
+    } else if constexpr (DIR == 1) {
+        if (t0 >= nx) return;
+        base = (long long)blockIdx.y * ny * nx + t0;
+        stride = nx;
+        len = ny;
+    } else {
+        if (t0 >= nx) return;
+        base = (long long)blockIdx.y * nx + t0;
+        stride = (long long)nx * ny;
+        len = nz;
+    }
+    const int c0 = blockIdx.z * seg;
+    if (c0 >= len) return;
+    const int c1 = min(c0 + seg, len);
+
+    const R gamma = R(P.gamma), eps = R(P.sw_eps);
+    R lin[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) lin[m] = R(P.lin[m]);
+    const R disp = R(P.mdcd_disp), diss = R(P.mdcd_diss);
+    const R inv_h = R(DIR == 0 ? P.inv_dx : (DIR == 1 ? P.inv_dy : P.inv_dz));
+
+    R fp[S][5], fm[S][5];
+    auto load_split = [&](int s, R* Fp, R* Fm) {
+        const long long id = base + (long long)wrap1(s, len) * stride;
+        R rr = R(W.rho[id]);
+        const R u = R(W.u[id]), v = R(W.v[id]), w = R(W.w[id]), p = R(W.p[id]);
+        if (rr <= R(0)) rr = R(1e-12);
+        R E, c;
+        p2c_Ec(rr, u, v, w, p, gamma, E, c);
+        if constexpr (FVS == FV_SW)
+            split_sw<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, gamma, eps, Fp, Fm);
+        else
+            split_lf<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fp, Fm);
+    };
+
+    int f = c0 - 1;  // face f sits between cells f and f+1 (the reference's i_face = f + ng)
+#pragma unroll
+    for (int m = 0; m < S - 1; ++m) load_split(f - MID + m, fp[m], fm[m]);
+    R prev[5];
+    for (int t = 0; f < c1; ++t, ++f) {
+        load_split(f - MID + S - 1, fp[S - 1], fm[S - 1]);
+        R face[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            R a[S], b[S];
+#pragma unroll
+            for (int m = 0; m < S; ++m) {
+                a[m] = fp[m][q];
+                b[m] = fm[S - 1 - m][q];  // reconstruct_select reverses for flag < 0
+            }
+            const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+            const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+            face[q] = plus_face + minus_face;
+        }
+        if (t > 0) {
+            const long long id = base + (long long)f * stride;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const R d = face[q] - prev[q];
+                if constexpr (DIR == 0)
+                    tacc[q * n + id] = d * inv_h;
+                else
+                    tacc[q * n + id] = tacc[q * n + id] + d * inv_h;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) prev[q] = face[q];
+#pragma unroll
+        for (int m = 0; m < S - 1; ++m)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                fp[m][q] = fp[m + 1][q];
+                fm[m][q] = fm[m + 1][q];
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Viscous flux (compute_gradients ViscousFlux.cpp:240-279 +
+// compute_viscous_flux :282-339). Output fv (type R), 9 blocks of n:
+//   0 tau_xx, 1 tau_yy, 2 tau_zz, 3 tau_xy, 4 tau_xz, 5 tau_yz,
+//   6 E-flux x, 7 E-flux y, 8 E-flux z.
+// The reference's 12 flux arrays map onto these (Fv = {xx, xy, xz, ex},
+// Hv = {xy, yy, yz, ey}, Gv = {xz, yz, zz, ez}); the mass fluxes are zero.
+// ---------------------------------------------------------------------------
+template <class R, int ORD>
+__global__ void __launch_bounds__(128)
+k_visc_flux(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict__ ctrl) {
+    if (ctrl && ctrl->stop) return;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx) return;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const long long n = P.n;
+    const long long id = ((long long)k * ny + j) * nx + i;
+    const long long sxy = (long long)nx * ny;
+    auto gx = [&](const double* a) {
+        return [=](int o) { return R(a[id + (wrap1(i + o, nx) - i)]); };
+    };
+    auto gy = [&](const double* a) {
+        return [=](int o) { return R(a[id + (long long)(wrap1(j + o, ny) - j) * nx]); };
+    };
+    auto gz = [&](const double* a) {
+        return [=](int o) { return R(a[id + (long long)(wrap1(k + o, nz) - k) * sxy]); };
+    };
+    const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
+    const R du_dx = dcentral<R, ORD>(gx(W.u), dx);
+    const R du_dy = dcentral<R, ORD>(gy(W.u), dy);
+    const R du_dz = dcentral<R, ORD>(gz(W.u), dz);
+    const R dv_dx = dcentral<R, ORD>(gx(W.v), dx);
+    const R dv_dy = dcentral<R, ORD>(gy(W.v), dy);
+    const R dv_dz = dcentral<R, ORD>(gz(W.v), dz);
+    const R dw_dx = dcentral<R, ORD>(gx(W.w), dx);
+    const R dw_dy = dcentral<R, ORD>(gy(W.w), dy);
+    const R dw_dz = dcentral<R, ORD>(gz(W.w), dz);
+    const R dT_dx = dcentral<R, ORD>(gx(W.T), dx);
+    const R dT_dy = dcentral<R, ORD>(gy(W.T), dy);
+    const R dT_dz = dcentral<R, ORD>(gz(W.T), dz);
+
+    const R mu = get_mu<R>(R(W.T[id]), R(P.mu), R(P.sutherland_s));
+    const R Cp = R(P.Cp), Pr = R(P.Pr);
+    const R divU = du_dx + dv_dy + dw_dz;
+    const R tau_xx = R(2.0) * mu * du_dx - R(2.0 / 3.0) * mu * divU;
+    const R tau_yy = R(2.0) * mu * dv_dy - R(2.0 / 3.0) * mu * divU;
+    const R tau_zz = R(2.0) * mu * dw_dz - R(2.0 / 3.0) * mu * divU;
+    const R tau_xy = mu * (du_dy + dv_dx);
+    const R tau_xz = mu * (du_dz + dw_dx);
+    const R tau_yz = mu * (dv_dz + dw_dy);
+    const R qx = mu * Cp / Pr * dT_dx;
+    const R qy = mu * Cp / Pr * dT_dy;
+    const R qz = mu * Cp / Pr * dT_dz;
+    const R u = R(W.u[id]), v = R(W.v[id]), w = R(W.w[id]);
+    fv[0 * n + id] = tau_xx;
+    fv[1 * n + id] = tau_yy;
+    fv[2 * n + id] = tau_zz;
+    fv[3 * n + id] = tau_xy;
+    fv[4 * n + id] = tau_xz;
+    fv[5 * n + id] = tau_yz;
+    fv[6 * n + id] = u * tau_xx + v * tau_xy + w * tau_xz + qx;
+    fv[7 * n + id] = u * tau_xy + v * tau_yy + w * tau_yz + qy;
+    fv[8 * n + id] = u * tau_xz + v * tau_yz + w * tau_zz + qz;
+}
+
+// rhs at one cell: compute_vis_flux (ViscousFlux.cpp:370-384, x then y then z
+// added to 0) followed by the inviscid divergence (range_kutta.cpp:61-97).
+template <class R, int ORD>
+__device__ __forceinline__ void cell_rhs(const DevParams& P, const R* __restrict__ tacc,
+                                         const R* __restrict__ fv, int i, int j, int k,
+                                         long long id, R r[5]) {
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = P.n, sxy = (long long)nx * ny;
+    auto gx = [&](int a) {
+        return [=](int o) { return fv[a * n + id + (wrap1(i + o, nx) - i)]; };
+    };
+    auto gy = [&](int a) {
+        return [=](int o) { return fv[a * n + id + (long long)(wrap1(j + o, ny) - j) * nx]; };
+    };
+    auto gz = [&](int a) {
+        return [=](int o) { return fv[a * n + id + (long long)(wrap1(k + o, nz) - k) * sxy]; };
+    };
+    const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
+    // flux blocks: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz, 6 ex, 7 ey, 8 ez
+    constexpr int FX[4] = {0, 3, 4, 6};  // Fv_momx, Fv_momy, Fv_momz, Fv_E
+    constexpr int FY[4] = {3, 1, 5, 7};  // Hv_*
+    constexpr int FZ[4] = {4, 5, 2, 8};  // Gv_*
+    r[0] = R(0.0);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        R acc = R(0.0);
+        acc += dcentral<R, ORD>(gx(FX[m]), dx);
+        acc += dcentral<R, ORD>(gy(FY[m]), dy);
+        acc += dcentral<R, ORD>(gz(FZ[m]), dz);
+        r[m + 1] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) r[q] += -tacc[q * n + id];
+}
+
+// compute_rhs output (5 blocks of n, double).
+template <class R, int ORD>
+__global__ void __launch_bounds__(128)
+k_rhs_out(DevParams P, const R* __restrict__ tacc, const R* __restrict__ fv,
+          double* __restrict__ rhs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nx) return;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const long long id = ((long long)k * P.ny + j) * P.nx + i;
+    R r[5];
+    cell_rhs<R, ORD>(P, tacc, fv, i, j, k, id, r);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) rhs[q * P.n + id] = double(r[q]);
+}
+
+// Conserved state of primitive cell values (primitiveToConserved).
+__device__ __forceinline__ void prim2cons_cell(const StateView& W, long long id, double gamma,
+                                               double U[5]) {
+    double rr = W.rho[id];
+    if (rr <= 0.0) rr = 1e-12;
+    const double u = W.u[id], v = W.v[id], w = W.w[id], p = W.p[id];
+    U[0] = rr;
+    U[1] = rr * u;
+    U[2] = rr * v;
+    U[3] = rr * w;
+    const double kinetic = 0.5 * (u * u + v * v + w * w);
+    const double e_internal = p / ((gamma - 1.0) * rr);
+    U[4] = rr * (e_internal + kinetic);
+}
+
+// Per-cell CFL candidate of compute_timestep (timestep.cpp:18-30), std::min
+// semantics (a NaN candidate never replaces the running minimum).
+__device__ __forceinline__ double cfl_candidate(const DevParams& P, double rho, double u,
+                                                double v, double w, double p) {
+    const double a = sqrt(P.gamma * p / (rho < 1e-14 ? 1e-14 : rho));
+    const double dt_x = P.dx / (fabs(u) + a);
+    const double dt_y = P.dy / (fabs(v) + a);
+    const double dt_z = P.dz / (fabs(w) + a);
+    double m = (dt_z < dt_y) ? dt_z : dt_y;
+    m = (m < dt_x) ? m : dt_x;
+    return m;
+}
+
+// Block-wide min of non-negative doubles, one atomicMin per block.
+__device__ __forceinline__ void block_min_to(double v, unsigned long long* dst) {
+    unsigned long long b = (v == v) ? pos_double_bits(v) : ~0ull;  // NaN never wins
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+        b = x < b ? x : b;
+    }
+    __shared__ unsigned long long red[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = b;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        b = lane < nw ? red[lane] : ~0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+            b = x < b ? x : b;
+        }
+        if (lane == 0 && b != ~0ull) atomicMin(dst, b);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage update (range_kutta.cpp:107-147) fused with the viscous divergence
+// and, after stage 3, the positivity check (:149-162) and the next step's CFL
+// candidates. Wc: current state, W0: recorded state (U0 = prim2cons(W0)),
+// Wn: output. Stage 3 may write Wn == W0 in place (each thread reads its own
+// cell of W0 before writing it), so no pointer here is __restrict__.
+// ---------------------------------------------------------------------------
+template <class R, int ORD, int STAGE>
+__global__ void __launch_bounds__(128)
+k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
+         const R* __restrict__ fv, StateOut Wn, Ctrl* ctrl) {
+    if (ctrl->stop) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < P.nx;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const long long id = ((long long)k * P.ny + j) * P.nx + (live ? i : 0);
+    double cand = CFL_INIT;
+    if (live) {
+        R r[5];
+        cell_rhs<R, ORD>(P, tacc, fv, i, j, k, id, r);
+        const double dt = ctrl->dt;
+        const double gamma = P.gamma;
+        double U0[5], U[5];
+        prim2cons_cell(W0, id, gamma, U0);
+        if (STAGE != 1) prim2cons_cell(Wc, id, gamma, U);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double rq = double(r[q]);
+            if (STAGE == 1)
+                U[q] = U0[q] + dt * rq;
+            else if (STAGE == 2)
+                U[q] = 0.75 * U0[q] + 0.25 * (U[q] + dt * rq);
+            else
+                U[q] = (1.0 / 3.0) * U0[q] + (2.0 / 3.0) * (U[q] + dt * rq);
+        }
+        // conservedToPrimitive (field_structures.h:405-427)
+        double rr = U[0];
+        if (rr <= 0.0) rr = 1e-12;
+        const double u = U[1] / rr, v = U[2] / rr, w = U[3] / rr;
+        const double kinetic = 0.5 * (u * u + v * v + w * w);
+        const double e_internal = U[4] / rr - kinetic;
+        const double p = (gamma - 1.0) * rr * e_internal;
+        const double T = p / (rr * P.Rgas);  // primitiveToConserved's T
+        Wn.rho[id] = rr;
+        Wn.u[id] = u;
+        Wn.v[id] = v;
+        Wn.w[id] = w;
+        Wn.p[id] = p;
+        Wn.T[id] = T;
+        if (STAGE == 3) {
+            if (rr <= 0.0 || p <= 0.0 || T <= 0.0) atomicMin(&ctrl->bad_cell, id);
+            cand = cfl_candidate(P, rr, u, v, w, p);
+        }
+    }
+    if (STAGE == 3) block_min_to(cand, &ctrl->dtmin_bits);
+}
+
+// Sums of the reductions below (see k_sums_partial).
+constexpr int NSUMS = 12;
+
+// The kernels from here on are not templates; only the API translation unit
+// (which defines NS3D_API_KERNELS) instantiates them.
+#ifdef NS3D_API_KERNELS
+
+// compute_timestep candidates of the current state (standalone).
+__global__ void __launch_bounds__(256)
+k_cfl(DevParams P, StateView W, Ctrl* ctrl) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double cand = CFL_INIT;
+    if (id < P.n) cand = cfl_candidate(P, W.rho[id], W.u[id], W.v[id], W.w[id], W.p[id]);
+    block_min_to(cand, &ctrl->dtmin_bits);
+}
+
+// Start of one time_advance iteration (maincycle.cpp:14-47). mode 0: plain
+// step (dt from CFL or dt_fixed); mode 1: with the TotalTime / output-time
+// clipping and stop conditions of time_advance.
+__global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, double total_time,
+                              double out_freq) {
+    if (c->stop) return;
+    const double eps = 1e-12;
+    if (mode == 1 && fabs(total_time - c->time) <= eps) {
+        c->stop = 1;
+        c->stop_reason = STOP_TOTAL_TIME;
+        c->stop_in_pre = 1;
+        c->active = 0;
+        return;
+    }
+    double dt = dt_fixed;
+    if (dt_fixed < 0.0) dt = cfl * __longlong_as_double((long long)c->dtmin_bits);
+    c->dtmin_bits = pos_double_bits(CFL_INIT);
+    if (mode == 1) {
+        double t = c->time;
+        if (t >= c->out_next - eps) c->out_next += out_freq;
+        if (t + dt > total_time) dt = total_time - t;
+        if (t + dt > c->out_next) {
+            dt = c->out_next - t;
+            c->out_next += out_freq;
+        }
+        if (dt <= eps) {
+            c->stop = 1;
+            c->stop_reason = STOP_DT_SMALL;
+            c->stop_in_pre = 1;
+            c->active = 0;
+            return;
+        }
+    }
+    c->time += dt;
+    c->dt = dt;
+    c->active = 1;
+}
+
+// End of one iteration (maincycle.cpp:250 + 298-300, range_kutta.cpp:149-162).
+__global__ void k_control_post(Ctrl* c, int mode, double total_time, long long n) {
+    if (c->stop || !c->active) return;
+    c->active = 0;
+    c->steps_done += 1;
+    if (c->bad_cell < n) {
+        c->stop = 1;
+        c->stop_reason = STOP_NONPHYSICAL;
+        return;
+    }
+    if (mode == 1 && c->time >= total_time) {
+        c->stop = 1;
+        c->stop_reason = STOP_TOTAL_TIME;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions (FP64)
+// ---------------------------------------------------------------------------
+
+// compute_total_energy (postprocess.cpp:103-128) and the sums of
+// compute_turbulence_statistics (ana_isotropic.cpp:241-255), per block, then
+// a second pass sums the block partials in double. Outputs 12 sums:
+// [0] sum 0.5 rho |u|^2, [1] sum 0.5|u|^2, [2] sum mu(T), [3] sum rho,
+// [4] sum |u|^2, [5..7] sum u,v,w, [8..10] sum u^2,v^2,w^2, [11] sum sqrt(g R T).
+
+__global__ void __launch_bounds__(256)
+k_sums_partial(DevParams P, StateView W, double* __restrict__ part) {
+    double s[NSUMS];
+#pragma unroll
+    for (int q = 0; q < NSUMS; ++q) s[q] = 0.0;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < P.n;
+         id += (long long)gridDim.x * blockDim.x) {
+        const double rho = W.rho[id], u = W.u[id], v = W.v[id], w = W.w[id], T = W.T[id];
+        const double q2 = u * u + v * v + w * w;
+        s[0] += 0.5 * rho * q2;
+        s[1] += 0.5 * q2;
+        s[2] += get_mu<double>(T, P.mu, P.sutherland_s);
+        s[3] += rho;
+        s[4] += q2;
+        s[5] += u;
+        s[6] += v;
+        s[7] += w;
+        s[8] += u * u;
+        s[9] += v * v;
+        s[10] += w * w;
+        s[11] += sqrt(P.gamma * P.Rgas * T);
+    }
+    __shared__ double red[NSUMS][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NSUMS; ++q) {
+        double x = s[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < NSUMS) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += red[threadIdx.x][w];
+        part[(long long)blockIdx.x * NSUMS + threadIdx.x] = x;
+    }
+}
+
+__global__ void k_sums_final(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
+    const int q = threadIdx.x;
+    if (q >= NSUMS) return;
+    double x = 0.0;
+    for (int b = 0; b < nblocks; ++b) x += part[(long long)b * NSUMS + q];
+    out[q] = x;
+}
+
+#endif  // NS3D_API_KERNELS
+
+}  // namespace ns3d

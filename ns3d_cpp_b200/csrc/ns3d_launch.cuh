@@ -1,0 +1,133 @@
+// Launchers for the stage kernels. Included by exactly one translation unit
+// per compute type (ns3d_fp64.cu: double, -fmad=false; ns3d_fp32.cu: float),
+// which instantiates them explicitly.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ns3d_kernels.cuh"
+
+namespace ns3d {
+
+struct LaunchCfg {
+    DevParams P;
+    int fvs;      // FV_SW / FV_LF
+    int rc;       // RC_* of the reconstruction
+    int seg[3];   // cells per thread segment along x, y, z
+    cudaStream_t stream;
+};
+
+// One inviscid sweep (dir 0, 1, 2 in this order per RHS evaluation).
+template <class R>
+cudaError_t launch_sweep(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl);
+template <class R>
+cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl);
+template <class R>
+cudaError_t launch_update(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
+                          const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl);
+template <class R>
+cudaError_t launch_rhs_out(const LaunchCfg& L, const R* tacc, const R* fv, double* rhs);
+
+#ifdef NS3D_LAUNCH_IMPL
+
+namespace detail {
+
+inline int threads_for(int ext) { return ext >= 128 ? 128 : (ext >= 64 ? 64 : 32); }
+
+template <int DIR, class R, int FVS, int RC>
+cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl) {
+    const DevParams& P = L.P;
+    const int ext = DIR == 0 ? P.ny : P.nx;        // thread dimension
+    const int other = DIR == 2 ? P.ny : P.nz;     // blockIdx.y dimension
+    const int len = DIR == 0 ? P.nx : (DIR == 1 ? P.ny : P.nz);
+    const int seg = L.seg[DIR] > 0 ? L.seg[DIR] : len;
+    const int th = threads_for(ext);
+    dim3 grid((ext + th - 1) / th, other, (len + seg - 1) / seg);
+    k_sweep<DIR, R, FVS, RC><<<grid, th, 0, L.stream>>>(P, W, tacc, seg, ctrl);
+    return cudaGetLastError();
+}
+
+template <class R, int FVS, int RC>
+cudaError_t sweeps(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl) {
+    if (dir == 0) return sweep_dir<0, R, FVS, RC>(L, W, tacc, ctrl);
+    if (dir == 1) return sweep_dir<1, R, FVS, RC>(L, W, tacc, ctrl);
+    return sweep_dir<2, R, FVS, RC>(L, W, tacc, ctrl);
+}
+
+template <class R, int FVS>
+cudaError_t sweeps_rc(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl) {
+    switch (L.rc) {
+    case RC_WENO5: return sweeps<R, FVS, RC_WENO5>(L, dir, W, tacc, ctrl);
+    case RC_LINEAR: return sweeps<R, FVS, RC_LINEAR>(L, dir, W, tacc, ctrl);
+    case RC_LIN6: return sweeps<R, FVS, RC_LIN6>(L, dir, W, tacc, ctrl);
+    case RC_MDCD_HYBRID: return sweeps<R, FVS, RC_MDCD_HYBRID>(L, dir, W, tacc, ctrl);
+    case RC_LIN8: return sweeps<R, FVS, RC_LIN8>(L, dir, W, tacc, ctrl);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+inline dim3 cell_grid(const DevParams& P, int th) { return dim3((P.nx + th - 1) / th, P.ny, P.nz); }
+
+}  // namespace detail
+
+template <class R>
+cudaError_t launch_sweep(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl) {
+    return L.fvs == FV_SW ? detail::sweeps_rc<R, FV_SW>(L, dir, W, tacc, ctrl)
+                          : detail::sweeps_rc<R, FV_LF>(L, dir, W, tacc, ctrl);
+}
+
+template <class R>
+cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl) {
+    const int th = detail::threads_for(L.P.nx);
+    const dim3 g = detail::cell_grid(L.P, th);
+    switch (L.P.vis_order) {
+    case 4: k_visc_flux<R, 4><<<g, th, 0, L.stream>>>(L.P, W, fv, ctrl); break;
+    case 6: k_visc_flux<R, 6><<<g, th, 0, L.stream>>>(L.P, W, fv, ctrl); break;
+    default: k_visc_flux<R, 8><<<g, th, 0, L.stream>>>(L.P, W, fv, ctrl); break;
+    }
+    return cudaGetLastError();
+}
+
+template <class R, int ORD>
+static cudaError_t update_ord(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
+                              const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl) {
+    const int th = detail::threads_for(L.P.nx);
+    const dim3 g = detail::cell_grid(L.P, th);
+    if (stage == 1) k_update<R, ORD, 1><<<g, th, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl);
+    else if (stage == 2) k_update<R, ORD, 2><<<g, th, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl);
+    else k_update<R, ORD, 3><<<g, th, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t launch_update(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
+                          const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl) {
+    switch (L.P.vis_order) {
+    case 4: return update_ord<R, 4>(L, stage, Wc, W0, tacc, fv, Wn, ctrl);
+    case 6: return update_ord<R, 6>(L, stage, Wc, W0, tacc, fv, Wn, ctrl);
+    default: return update_ord<R, 8>(L, stage, Wc, W0, tacc, fv, Wn, ctrl);
+    }
+}
+
+template <class R>
+cudaError_t launch_rhs_out(const LaunchCfg& L, const R* tacc, const R* fv, double* rhs) {
+    const int th = detail::threads_for(L.P.nx);
+    const dim3 g = detail::cell_grid(L.P, th);
+    switch (L.P.vis_order) {
+    case 4: k_rhs_out<R, 4><<<g, th, 0, L.stream>>>(L.P, tacc, fv, rhs); break;
+    case 6: k_rhs_out<R, 6><<<g, th, 0, L.stream>>>(L.P, tacc, fv, rhs); break;
+    default: k_rhs_out<R, 8><<<g, th, 0, L.stream>>>(L.P, tacc, fv, rhs); break;
+    }
+    return cudaGetLastError();
+}
+
+#define NS3D_INSTANTIATE_LAUNCHERS(R)                                                          \
+    template cudaError_t launch_sweep<R>(const LaunchCfg&, int, StateView, R*, const Ctrl*);   \
+    template cudaError_t launch_visc_flux<R>(const LaunchCfg&, StateView, R*, const Ctrl*);    \
+    template cudaError_t launch_update<R>(const LaunchCfg&, int, StateView, StateView,         \
+                                          const R*, const R*, StateOut, Ctrl*);                \
+    template cudaError_t launch_rhs_out<R>(const LaunchCfg&, const R*, const R*, double*);
+
+#endif  // NS3D_LAUNCH_IMPL
+
+}  // namespace ns3d

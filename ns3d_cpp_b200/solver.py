@@ -1,0 +1,288 @@
+"""Python host mirror of the reference's solver interface over the C ABI.
+
+Names follow the reference: :class:`SolverParams` (field_structures.h:85-166),
+:func:`read_solver_params_from_file` (initialization.cpp:199), and on
+:class:`Solver` the operations of Field3D / range_kutta / timestep /
+maincycle: ``record_conserved0`` (recordConservedTo0), ``compute_rhs``,
+``compute_timestep``, ``runge_kutta_3``, ``time_advance``,
+``compute_total_energy``, ``compute_energy_spectrum``,
+``compute_turbulence_statistics``.
+
+Everything runs in ``libns3d_b200.so`` on the GPU; there is no CPU fallback.
+Where the reference aborts (MPI_Abort on a non-physical state) or throws,
+these methods raise :class:`NS3DError` carrying the C status code.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+
+STATUS = {0: "OK", 1: "ERR_INVALID", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4: "ERR_NONPHYSICAL",
+          5: "ERR_FILE", 6: "ERR_DT", 7: "ERR_NOMEM", 8: "ERR_TIMEOUT"}
+
+FVS = {"stagerwarming": 0, "laxfriedrichs": 1}
+RECON = {"weno5": 0, "wcns": 1, "linear": 2, "mdcd": 3, "mdcd_hybrid": 4, "upwind_7th": 5,
+         "ud7l": 6}
+VIS = {"c8th": 0, "c6th": 1, "c4th": 2}
+PRECISION = {"fp64": 0, "fp32acc64": 1}
+LAYOUT = {"interior": 0, "ghosted": 1}
+
+
+class NS3DError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = int(status)
+        super().__init__(f"{STATUS.get(self.status, self.status)}: {message}")
+
+
+class SolverParams(ctypes.Structure):
+    """``ns3d_params`` of include/ns3d_gpu.h (SolverParams + GridDesc)."""
+    _fields_ = [
+        ("gamma", ctypes.c_double), ("Pr", ctypes.c_double), ("Ma", ctypes.c_double),
+        ("Re", ctypes.c_double), ("cfl", ctypes.c_double), ("dt_fixed", ctypes.c_double),
+        ("fvs_type", ctypes.c_int), ("recon", ctypes.c_int), ("vis_scheme", ctypes.c_int),
+        ("char_recon", ctypes.c_int),
+        ("mdcd_diss", ctypes.c_double), ("mdcd_disp", ctypes.c_double),
+        ("ud7l_alpha", ctypes.c_double),
+        ("global_nx", ctypes.c_int), ("global_ny", ctypes.c_int), ("global_nz", ctypes.c_int),
+        ("x0", ctypes.c_double), ("y0", ctypes.c_double), ("z0", ctypes.c_double),
+        ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double),
+        ("bc", ctypes.c_int * 6),
+        ("max_steps", ctypes.c_int), ("monitor_Stepfreq", ctypes.c_int),
+        ("output_Timefreq", ctypes.c_double), ("TotalTime", ctypes.c_double),
+        ("post_basicfield", ctypes.c_int), ("isotropic_analyse", ctypes.c_int),
+        ("monitor_res", ctypes.c_int), ("monitor_energy", ctypes.c_int),
+        ("Cv", ctypes.c_double), ("Cp", ctypes.c_double), ("Rgas", ctypes.c_double),
+        ("mu", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("dz", ctypes.c_double),
+        ("stencil", ctypes.c_int), ("ghost_layers", ctypes.c_int), ("periods", ctypes.c_int * 3),
+        ("sw_entropy_eps", ctypes.c_double), ("sutherland_s_over_tref", ctypes.c_double),
+        ("precision", ctypes.c_int), ("reserved", ctypes.c_int * 7),
+    ]
+
+    @classmethod
+    def default(cls) -> "SolverParams":
+        p = cls()
+        _check(_lib.load().ns3d_params_default(ctypes.byref(p)))
+        return p
+
+    def derive(self) -> "SolverParams":
+        _check(_lib.load().ns3d_params_derive(ctypes.byref(self)))
+        return self
+
+    def copy(self) -> "SolverParams":
+        p = SolverParams()
+        ctypes.memmove(ctypes.byref(p), ctypes.byref(self), ctypes.sizeof(self))
+        return p
+
+    def replace(self, **kw) -> "SolverParams":
+        """A derived copy with fields changed; enum fields accept the solver.in
+        spellings (e.g. recon="weno5", precision="fp32acc64")."""
+        p = self.copy()
+        for k, v in kw.items():
+            if isinstance(v, str):
+                table = {"fvs_type": FVS, "recon": RECON, "vis_scheme": VIS,
+                         "precision": PRECISION}[k]
+                v = table[v.lower()]
+            if k == "n":
+                p.global_nx = p.global_ny = p.global_nz = int(v)
+                continue
+            setattr(p, k, v)
+        return p.derive()
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, typ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class TurbStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("kinetic_energy", "tke", "u_rms", "dissipation", "nu", "mean_mu", "mean_rho",
+                 "mach_t", "total_energy")] + [("reserved", ctypes.c_double * 7)]
+
+
+def _check(status: int, ctx=None) -> None:
+    if status != 0:
+        msg = ""
+        if ctx is not None:
+            msg = _lib.load().ns3d_last_error(ctx).decode(errors="replace")
+        raise NS3DError(status, msg)
+
+
+def read_solver_params_from_file(path: str) -> SolverParams:
+    """read_solver_params_from_file (initialization.cpp:199-380)."""
+    p = SolverParams()
+    st = _lib.load().ns3d_params_from_file(os.fsencode(path), ctypes.byref(p))
+    if st != 0:
+        raise NS3DError(st, f"cannot read {path}")
+    return p
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """One resident periodic domain on one GPU (ns3d_ctx)."""
+
+    def __init__(self, params: SolverParams, device: int = 0):
+        self.lib = _lib.load()
+        self.params = params.copy().derive()
+        self.ctx = ctypes.c_void_p()
+        st = self.lib.ns3d_create(ctypes.byref(self.params), int(device), ctypes.byref(self.ctx))
+        if st != 0:
+            raise NS3DError(st, "ns3d_create failed")
+        p = self.params
+        self.shape = (p.global_nz, p.global_ny, p.global_nx)
+        g = p.ghost_layers
+        self.ghosted_shape = (p.global_nz + 2 * g, p.global_ny + 2 * g, p.global_nx + 2 * g)
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.ns3d_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, st: int) -> None:
+        _check(st, self.ctx)
+
+    # -- state --------------------------------------------------------------
+    def _prep(self, arrays, layout: str):
+        shape = self.shape if layout == "interior" else self.ghosted_shape
+        out = []
+        for a in arrays:
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            if a.shape != shape:
+                raise ValueError(f"array of shape {a.shape}, expected {shape}")
+            out.append(a)
+        return out
+
+    def upload_primitive(self, W, layout: str = "interior") -> None:
+        """Initial condition path (main.cpp:67-71); also records U0."""
+        arrs = self._prep(W, layout)
+        self._ck(self.lib.ns3d_upload_primitive(self.ctx, *[_dptr(a) for a in arrs],
+                                                LAYOUT[layout]))
+
+    def upload_conserved(self, U, layout: str = "interior") -> None:
+        """conservedToPrimitive + apply_boundary + primitiveToConserved; records U0."""
+        arrs = self._prep(U, layout)
+        self._ck(self.lib.ns3d_upload_conserved(self.ctx, *[_dptr(a) for a in arrs],
+                                                LAYOUT[layout]))
+
+    def download_primitive(self, layout: str = "interior", with_T_c: bool = False):
+        shape = self.shape if layout == "interior" else self.ghosted_shape
+        out = np.empty((7 if with_T_c else 5,) + shape)
+        ptrs = [_dptr(out[q]) for q in range(out.shape[0])]
+        if not with_T_c:
+            ptrs += [None, None]
+        self._ck(self.lib.ns3d_download_primitive(self.ctx, *ptrs, LAYOUT[layout]))
+        return out
+
+    def download_conserved(self, layout: str = "interior"):
+        shape = self.shape if layout == "interior" else self.ghosted_shape
+        out = np.empty((5,) + shape)
+        self._ck(self.lib.ns3d_download_conserved(self.ctx, *[_dptr(out[q]) for q in range(5)],
+                                                  LAYOUT[layout]))
+        return out
+
+    # -- hot path -----------------------------------------------------------
+    def record_conserved0(self) -> None:
+        self._ck(self.lib.ns3d_record_conserved0(self.ctx))
+
+    def compute_rhs(self, layout: str = "interior"):
+        shape = self.shape if layout == "interior" else self.ghosted_shape
+        out = np.empty((5,) + shape)
+        self._ck(self.lib.ns3d_compute_rhs(self.ctx, *[_dptr(out[q]) for q in range(5)],
+                                           LAYOUT[layout]))
+        return out
+
+    def compute_timestep(self) -> float:
+        dt = ctypes.c_double()
+        self._ck(self.lib.ns3d_compute_timestep(self.ctx, ctypes.byref(dt)))
+        return dt.value
+
+    def runge_kutta_3(self, dt: float) -> None:
+        self._ck(self.lib.ns3d_runge_kutta_3(self.ctx, float(dt)))
+
+    def time_advance(self, max_steps: int):
+        """Returns (current_time, steps_done)."""
+        t = ctypes.c_double()
+        k = ctypes.c_int()
+        self._ck(self.lib.ns3d_time_advance(self.ctx, int(max_steps), ctypes.byref(t),
+                                            ctypes.byref(k)))
+        return t.value, k.value
+
+    def step(self, nsteps: int = 1) -> None:
+        self._ck(self.lib.ns3d_step(self.ctx, int(nsteps)))
+
+    def last_dt(self) -> float:
+        dt = ctypes.c_double()
+        self._ck(self.lib.ns3d_last_dt(self.ctx, ctypes.byref(dt)))
+        return dt.value
+
+    def synchronize(self) -> None:
+        self._ck(self.lib.ns3d_synchronize(self.ctx))
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        self._ck(self.lib.ns3d_device_bytes(self.ctx, ctypes.byref(b)))
+        return b.value
+
+    # -- instrumentation ----------------------------------------------------
+    KERNEL_CLASSES = ("sweep_x", "sweep_y", "sweep_z", "visc_flux", "update", "other")
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t (as an int) all kernels of this context run on."""
+        s = ctypes.c_void_p()
+        self._ck(self.lib.ns3d_get_stream(self.ctx, ctypes.byref(s)))
+        return s.value or 0
+
+    def profile(self, enable: bool) -> None:
+        self._ck(self.lib.ns3d_profile(self.ctx, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        ms = (ctypes.c_double * 6)()
+        n = (ctypes.c_longlong * 6)()
+        self._ck(self.lib.ns3d_profile_read(self.ctx, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def launch_count(self) -> int:
+        c = ctypes.c_longlong()
+        self._ck(self.lib.ns3d_launch_count(self.ctx, ctypes.byref(c)))
+        return c.value
+
+    # -- reductions ---------------------------------------------------------
+    def compute_total_energy(self) -> float:
+        e = ctypes.c_double()
+        self._ck(self.lib.ns3d_total_energy(self.ctx, ctypes.byref(e)))
+        return e.value
+
+    def compute_energy_spectrum(self, nbins: int | None = None):
+        if nbins is None:
+            nbins = 2 * self.params.global_nx + 1
+        out = np.empty(nbins)
+        self._ck(self.lib.ns3d_energy_spectrum(self.ctx, _dptr(out), int(nbins)))
+        return out
+
+    def compute_turbulence_statistics(self) -> dict:
+        s = TurbStats()
+        self._ck(self.lib.ns3d_turbulence_stats(self.ctx, ctypes.byref(s)))
+        return {n: getattr(s, n) for n, _ in TurbStats._fields_ if n != "reserved"}

@@ -176,6 +176,16 @@ static void split_lf(const orc_params *P, double rho, double u, double v, double
     Fm[4] = 0.5 * (F5 - a_max * E);
 }
 
+/* Split fluxes of one cell state (rho,u,v,w,p) along direction dir. */
+void orc_split(const orc_params *P, const double *w5, int dir, double *Fp, double *Fm) {
+    double rr = w5[0], ru, rv, rw, E, T, c;
+    p2c(P, rr, w5[1], w5[2], w5[3], w5[4], &ru, &rv, &rw, &E, &T, &c);
+    if (P->fvs == ORC_SW)
+        split_sw(P, rr, w5[1], w5[2], w5[3], E, w5[4], c, dir == 0, dir == 1, dir == 2, Fp, Fm);
+    else
+        split_lf(P, rr, w5[1], w5[2], w5[3], E, w5[4], c, dir == 0, dir == 1, dir == 2, Fp, Fm);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Scalar reconstructions: reconstruction.cpp                               */
 /* ------------------------------------------------------------------------ */

@@ -125,6 +125,7 @@ def _orc_lib():
         lib.orc_turb_sums.argtypes = [P, D, D]
         lib.orc_recon_scalar.argtypes = [P, D, ctypes.c_int, ctypes.c_double]
         lib.orc_recon_scalar.restype = ctypes.c_double
+        lib.orc_split.argtypes = [P, D, ctypes.c_int, D, D]
         _ORC = lib
     return _ORC
 
@@ -204,6 +205,47 @@ class Oracle:
         out = np.zeros(11)
         self.lib.orc_turb_sums(ctypes.byref(self.p), _dp(self._w(W)), _dp(out))
         return out
+
+    def split(self, w5, direction):
+        """(F+, F-) of one cell state (rho,u,v,w,p) along `direction`."""
+        a = np.ascontiguousarray(w5, dtype=np.float64)
+        fp = np.empty(5)
+        fm = np.empty(5)
+        self.lib.orc_split(ctypes.byref(self.p), _dp(a), int(direction), _dp(fp), _dp(fm))
+        return fp, fm
+
+    def time_advance(self, W, max_steps, total_time, output_timefreq):
+        """The step loop of time_advance (maincycle.cpp:12-50) without monitor
+        output: returns (W, current_time, steps_done, dts)."""
+        eps = 1e-12
+        t = 0.0
+        out_next = output_timefreq
+        dts = []
+        steps = 0
+        for _step in range(1, max_steps + 1):
+            if abs(total_time - t) <= eps:
+                break
+            dt = self.d["dt_fixed"]
+            if self.d["dt_fixed"] < 0.0:
+                dt = self.timestep(W)
+            if t >= out_next - eps:
+                out_next += output_timefreq
+            if t + dt > total_time:
+                dt = total_time - t
+            if t + dt > out_next:
+                dt = out_next - t
+                out_next += output_timefreq
+            if dt <= eps:
+                break
+            t += dt
+            W, st = self.rk3(W, dt)
+            dts.append(dt)
+            steps += 1
+            if st:
+                raise RuntimeError("non-physical state")
+            if t >= total_time:
+                break
+        return W, t, steps, dts
 
     def recon_scalar(self, window, flag):
         a = np.ascontiguousarray(window, dtype=np.float64)

@@ -1,0 +1,219 @@
+"""GPU (B200) parity of the CUDA path against the oracle, through the C ABI.
+
+Tolerances: FP64 form 1e-12 norm-wise relative (max|a-b|/max|b| per
+variable); FP32-stencil form against the FP64 oracle as stated per test.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import ns3d_cpp_b200 as ns
+from ns3d_cpp_b200 import initial
+from conftest import SCHEMES, ref_cfg, relerr, scheme_id
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+
+def params_from_cfg(cfg, **extra):
+    """Parse a reference-format solver.in through the library's parser."""
+    text = "".join(f"{k} = {v}\n" for k, v in {**cfg, **extra}.items())
+    with tempfile.NamedTemporaryFile("w", suffix=".in", delete=False) as f:
+        f.write(text)
+        path = f.name
+    try:
+        return ns.read_solver_params_from_file(path)
+    finally:
+        os.unlink(path)
+
+
+def tgv_input(n, seed=11):
+    return initial.taylor_green(n, Ma=0.1, perturb=0.05, seed=seed)
+
+
+@pytest.mark.parametrize("kw", SCHEMES, ids=scheme_id)
+def test_rhs_fp64_matches_oracle(oracle_mod, kw):
+    n = 16
+    cfg = ref_cfg(n, **kw)
+    W = tgv_input(n)
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        rhs = s.compute_rhs()
+    ref = oracle_mod.Oracle(cfg).rhs(W)
+    err = relerr(rhs, ref)
+    assert np.all(err <= TOL64), err
+
+
+@pytest.mark.parametrize("kw", SCHEMES, ids=scheme_id)
+def test_cfl_steps_fp64_match_oracle(oracle_mod, kw):
+    n = 12
+    cfg = ref_cfg(n, **kw)
+    W = tgv_input(n, seed=3)
+    o = oracle_mod.Oracle(cfg)
+    Wo = W
+    dts = []
+    for _ in range(5):
+        Wo, dt, st = o.cfl_step(Wo)
+        assert st == 0
+        dts.append(dt)
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        s.step(5)
+        assert abs(s.last_dt() - dts[-1]) <= 1e-14 * dts[-1]
+        Wg = s.download_primitive()
+    assert np.all(relerr(Wg, Wo) <= TOL64)
+
+
+def test_timestep_and_runge_kutta_3_entry_points(oracle_mod):
+    n = 16
+    cfg = ref_cfg(n)
+    W = tgv_input(n, seed=5)
+    o = oracle_mod.Oracle(cfg)
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        dt = s.compute_timestep()
+        assert dt == o.timestep(W)
+        s.record_conserved0()
+        s.runge_kutta_3(dt)
+        Wg = s.download_primitive()
+        Ug = s.download_conserved()
+    W1, st = o.rk3(W, dt)
+    assert st == 0
+    assert np.all(relerr(Wg, W1) <= TOL64)
+    assert np.all(relerr(Ug, o.prim2cons(W1)[0]) <= TOL64)
+
+
+def test_time_advance_clipping_matches_oracle(oracle_mod):
+    n = 8
+    cfg = ref_cfg(n, TotalTime=0.05, output_Timefreq=0.0123)
+    W = initial.taylor_green(n, Ma=0.1)
+    o = oracle_mod.Oracle(cfg)
+    W2, t, steps, dts = o.time_advance(W, 40, 0.05, 0.0123)
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        tg, kg = s.time_advance(40)
+        Wg = s.download_primitive()
+        # already at TotalTime: a further call takes no step
+        tg2, kg2 = s.time_advance(5)
+    assert kg == steps and abs(tg - t) <= 1e-15
+    assert kg2 == 0 and tg2 == tg
+    assert np.all(relerr(Wg, W2) <= TOL64)
+
+
+def test_nonphysical_state_returns_status():
+    """A negative pressure injected on the host: runge_kutta_3 reports
+    NS3D_ERR_NONPHYSICAL (the reference calls MPI_Abort)."""
+    n = 8
+    W = initial.taylor_green(n, Ma=0.1)
+    W[4, 3, 2, 1] = -5.0
+    with ns.Solver(params_from_cfg(ref_cfg(n))) as s:
+        s.upload_primitive(W)
+        with pytest.raises(ns.NS3DError) as e:
+            s.runge_kutta_3(1e-4)
+        assert e.value.status == 4
+        # the context stays usable
+        s.upload_primitive(initial.taylor_green(n, Ma=0.1))
+        s.runge_kutta_3(1e-4)
+
+
+def test_conserved_upload_and_ghosted_layout(oracle_mod):
+    n = 8
+    cfg = ref_cfg(n)
+    W = tgv_input(n, seed=2)
+    o = oracle_mod.Oracle(cfg)
+    U = o.prim2cons(W)[0]
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_conserved(U)
+        Wg = s.download_primitive()
+        assert np.array_equal(Wg, o.cons2prim(U))
+        G = s.download_primitive(layout="ghosted", with_T_c=True)
+        Gc = s.download_conserved(layout="ghosted")
+        # interior of the ghosted download is the state; ghosts are periodic images
+        g = s.params.ghost_layers
+        assert np.array_equal(G[:5, g:-g, g:-g, g:-g], Wg)
+        assert np.array_equal(G[1, g:-g, g:-g, :g], Wg[1, :, :, -g:])
+        assert np.all(G[0, :g, :g, :] == 1.0) and np.all(G[4, :g, :g, :] == 0.0)
+        # a ghosted upload reads the interior only
+        s.upload_primitive(G[:5], layout="ghosted")
+        assert np.array_equal(s.download_primitive(), Wg)
+        s.upload_conserved(Gc, layout="ghosted")
+        assert np.array_equal(s.download_primitive(), Wg)
+    if oracle_mod.have_ref():
+        r = oracle_mod.Ref(cfg)
+        r.set_conserved(U)
+        for q, name in enumerate(("rho", "u", "v", "w", "p", "T", "c")):
+            full = np.empty(G.shape[1:])
+            r.lib.ref_get_full(r.h, name.encode(), oracle_mod._dp(full))
+            # faces of the Field3D arrays: identical; edges/corners: never read
+            sl = (slice(g, -g), slice(g, -g))
+            assert np.array_equal(G[q][:, sl[0], sl[1]], full[:, sl[0], sl[1]]), name
+
+
+def test_reductions_match_oracle(oracle_mod):
+    n = 32
+    cfg = ref_cfg(n, Ma=0.5, Re=500)
+    W = initial.isotropic(n, mach_t=0.3, Ma=0.5, seed=4)
+    o = oracle_mod.Oracle(cfg)
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        ke = s.compute_total_energy()
+        Ek = s.compute_energy_spectrum()
+        st = s.compute_turbulence_statistics()
+    assert abs(ke - o.total_energy(W)) <= 1e-13 * ke
+    Eo = oracle_mod.spectrum(W[1], W[2], W[3])
+    big = Eo > 1e-14 * Eo.max()
+    np.testing.assert_allclose(Ek[big], Eo[big], rtol=1e-11)
+    so = oracle_mod.turbulence_stats(o.turb_sums(W), Eo, n ** 3, o.d["gamma"], o.d["Rgas"])
+    for k in ("kinetic_energy", "tke", "u_rms", "dissipation", "nu"):
+        assert abs(st[k] - so[k]) <= 1e-11 * abs(so[k]), k
+    assert abs(st["mach_t"] - 0.3) < 1e-12
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(fvs_type="LaxFriedrichs", recon="MDCD"),
+                                dict(recon="UPWIND_7TH")], ids=scheme_id)
+def test_fp32_stencils_close_to_fp64(oracle_mod, kw):
+    """FP32-stencil form: RHS within 1e-5 and 10 steps within 1e-6 of FP64."""
+    n = 16
+    cfg = ref_cfg(n, **kw)
+    W = tgv_input(n, seed=9)
+    o = oracle_mod.Oracle(cfg)
+    with ns.Solver(params_from_cfg(cfg, precision="fp32acc64")) as s:
+        s.upload_primitive(W)
+        rhs = s.compute_rhs()
+        s.step(10)
+        Wg = s.download_primitive()
+    assert np.all(relerr(rhs, o.rhs(W)) <= 1e-5)
+    Wo = W
+    for _ in range(10):
+        Wo, _, st = o.cfl_step(Wo)
+    assert np.all(relerr(Wg, Wo) <= 1e-6)
+
+
+def test_rhs_fp64_64_matches_oracle(oracle_mod):
+    n = 64
+    cfg = ref_cfg(n, Ma=0.5, Re=500, fvs_type="LaxFriedrichs", recon="MDCD")
+    W = initial.isotropic(n, mach_t=0.3, Ma=0.5, seed=1)
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        rhs = s.compute_rhs()
+    assert np.all(relerr(rhs, oracle_mod.Oracle(cfg).rhs(W)) <= TOL64)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32acc64"])
+def test_full_size_properties(precision):
+    """256^3 (the benchmark size): periodic translation invariance is exact
+    (every cell runs the same operations), and the mass equation telescopes."""
+    n = 256
+    cfg = ref_cfg(n, Ma=0.5, Re=1000)
+    W = initial.isotropic(n, mach_t=0.5, Ma=0.5, seed=2)
+    with ns.Solver(params_from_cfg(cfg, precision=precision)) as s:
+        s.upload_primitive(W)
+        r1 = s.compute_rhs()
+        s.upload_primitive(np.roll(W, (3, -5, 7), axis=(1, 2, 3)))
+        r2 = s.compute_rhs()
+    assert np.array_equal(np.roll(r1, (3, -5, 7), axis=(1, 2, 3)), r2)
+    mass = abs(r1[0].sum()) / np.abs(r1[0]).sum()
+    assert mass < (1e-12 if precision == "fp64" else 1e-5)
