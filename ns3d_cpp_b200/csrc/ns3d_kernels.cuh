@@ -105,25 +105,62 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     const R inv_h = R(DIR == 0 ? P.inv_dx : (DIR == 1 ? P.inv_dy : P.inv_dz));
 
     R fp[S][5], fm[S][5];
-    auto load_split = [&](int s, R* Fp, R* Fm) {
+    // FP32-stencil form: the split is evaluated in double from the double
+    // state and the segment's first split flux is subtracted before rounding
+    // to float, so the float reconstruction works on deviations of size
+    // O(variation) instead of O(value) (p ~ 1/(gamma Ma^2) otherwise leaves
+    // ~1e-4 relative error in pressure gradients). Every reconstruction is
+    // shift-invariant (weights from differences, coefficients summing to 1)
+    // and the offset is the same for both faces of a cell, so it cancels in the
+    // face-flux difference. The FP64 form keeps the reference's arithmetic.
+    constexpr bool kDeviation = sizeof(R) < sizeof(double);
+    double refp[5], refm[5];
+    auto load_split = [&](int s, R* Fp, R* Fm, bool set_ref) {
         const long long id = base + (long long)wrap1(s, len) * stride;
-        R rr = R(W.rho[id]);
-        const R u = R(W.u[id]), v = R(W.v[id]), w = R(W.w[id]), p = R(W.p[id]);
-        if (rr <= R(0)) rr = R(1e-12);
-        R E, c;
-        p2c_Ec(rr, u, v, w, p, gamma, E, c);
-        if constexpr (FVS == FV_SW)
-            split_sw<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, gamma, eps, Fp, Fm);
-        else
-            split_lf<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fp, Fm);
+        if constexpr (!kDeviation) {
+            R rr = R(W.rho[id]);
+            const R u = R(W.u[id]), v = R(W.v[id]), w = R(W.w[id]), p = R(W.p[id]);
+            if (rr <= R(0)) rr = R(1e-12);
+            R E, c;
+            p2c_Ec(rr, u, v, w, p, gamma, E, c);
+            if constexpr (FVS == FV_SW)
+                split_sw<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, gamma, eps, Fp, Fm);
+            else
+                split_lf<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fp, Fm);
+        } else {
+            double rr = W.rho[id];
+            const double u = W.u[id], v = W.v[id], w = W.w[id], p = W.p[id];
+            if (rr <= 0.0) rr = 1e-12;
+            double E, c, Fpd[5], Fmd[5];
+            p2c_Ec<double>(rr, u, v, w, p, P.gamma, E, c);
+            if constexpr (FVS == FV_SW)
+                split_sw<double, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, P.gamma,
+                                                               P.sw_eps, Fpd, Fmd);
+            else
+                split_lf<double, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fpd, Fmd);
+            if (set_ref) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    refp[q] = Fpd[q];
+                    refm[q] = Fmd[q];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                Fp[q] = R(Fpd[q] - refp[q]);
+                Fm[q] = R(Fmd[q] - refm[q]);
+            }
+        }
     };
+    (void)gamma;
+    (void)eps;
 
     int f = c0 - 1;  // face f sits between cells f and f+1 (the reference's i_face = f + ng)
 #pragma unroll
-    for (int m = 0; m < S - 1; ++m) load_split(f - MID + m, fp[m], fm[m]);
+    for (int m = 0; m < S - 1; ++m) load_split(f - MID + m, fp[m], fm[m], m == 0);
     R prev[5];
     for (int t = 0; f < c1; ++t, ++f) {
-        load_split(f - MID + S - 1, fp[S - 1], fm[S - 1]);
+        load_split(f - MID + S - 1, fp[S - 1], fm[S - 1], S == 1);
         R face[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -179,14 +216,21 @@ k_visc_flux(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict
     const long long n = P.n;
     const long long id = ((long long)k * ny + j) * nx + i;
     const long long sxy = (long long)nx * ny;
+    // FP32-stencil form: differentiate deviations from the centre value, formed
+    // in double (the central stencils' coefficients sum to zero, so the
+    // derivative is unchanged while T ~ 1 +- small keeps its low-order digits).
+    constexpr bool kDeviation = sizeof(R) < sizeof(double);
     auto gx = [&](const double* a) {
-        return [=](int o) { return R(a[id + (wrap1(i + o, nx) - i)]); };
+        const double c0 = kDeviation ? a[id] : 0.0;
+        return [=](int o) { return R(a[id + (wrap1(i + o, nx) - i)] - c0); };
     };
     auto gy = [&](const double* a) {
-        return [=](int o) { return R(a[id + (long long)(wrap1(j + o, ny) - j) * nx]); };
+        const double c0 = kDeviation ? a[id] : 0.0;
+        return [=](int o) { return R(a[id + (long long)(wrap1(j + o, ny) - j) * nx] - c0); };
     };
     auto gz = [&](const double* a) {
-        return [=](int o) { return R(a[id + (long long)(wrap1(k + o, nz) - k) * sxy]); };
+        const double c0 = kDeviation ? a[id] : 0.0;
+        return [=](int o) { return R(a[id + (long long)(wrap1(k + o, nz) - k) * sxy] - c0); };
     };
     const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
     const R du_dx = dcentral<R, ORD>(gx(W.u), dx);
@@ -378,7 +422,9 @@ k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
         Wn.p[id] = p;
         Wn.T[id] = T;
         if (STAGE == 3) {
-            if (rr <= 0.0 || p <= 0.0 || T <= 0.0) atomicMin(&ctrl->bad_cell, id);
+            // range_kutta.cpp:154 tests rho <= 0 || p <= 0 || T <= 0, which a
+            // NaN passes; the negated form below also reports NaN.
+            if (!(rr > 0.0) || !(p > 0.0) || !(T > 0.0)) atomicMin(&ctrl->bad_cell, id);
             cand = cfl_candidate(P, rr, u, v, w, p);
         }
     }
