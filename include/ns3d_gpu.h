@@ -9,8 +9,8 @@
  *
  * Each entry point names the reference function it replaces (file:line in
  * wylx-2/ns3d_cpp). The reference's C++ signatures (compute_rhs,
- * runge_kutta_3, compute_timestep, time_advance over Field3D) are provided on
- * top of this ABI by the shim described in INTEGRATION.md.
+ * runge_kutta_3, compute_timestep over Field3D) are provided on top of this
+ * ABI by the C++ shim ns3d_cpp_b200/shim/ns3d_shim.cpp.
  *
  * Arrays cross the boundary in one of two layouts (x fastest in both):
  *   NS3D_LAYOUT_INTERIOR  nx*ny*nz, a[(k*ny + j)*nx + i]
@@ -29,7 +29,8 @@ extern "C" {
 typedef enum ns3d_status {
     NS3D_OK = 0,
     NS3D_ERR_INVALID = 1,      /* bad argument or configuration */
-    NS3D_ERR_UNSUPPORTED = 2,  /* valid in the reference, not built here */
+    NS3D_ERR_UNSUPPORTED = 2,  /* valid in the reference, not built here: non-periodic
+                                  boundaries, char_recon, WCNS */
     NS3D_ERR_CUDA = 3,         /* CUDA runtime / cuFFT failure */
     NS3D_ERR_NONPHYSICAL = 4,  /* rho, p or T <= 0 after a step (range_kutta.cpp:149-162) */
     NS3D_ERR_FILE = 5,         /* solver.in cannot be opened (initialization.cpp:206-209) */

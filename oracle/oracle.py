@@ -44,6 +44,9 @@ def build(ref: bool | None = None) -> None:
         ref = os.path.isdir(REF_DIR)
     if ref:
         targets.append("ref")
+        gpu_lib = os.path.join(os.path.dirname(HERE), "ns3d_cpp_b200", "libns3d_b200.so")
+        if os.path.exists(gpu_lib):
+            targets.append("refgpu")
     subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={REF_DIR}", "-j8", *targets], check=True)
 
 
@@ -256,13 +259,15 @@ class Oracle:
 # The reference itself (compiled from its sources)
 # --------------------------------------------------------------------------
 
-_REF = None
+_REF = {}
+# the reference's sources with range_kutta.cpp / timestep.cpp replaced by the
+# product's C++ shim (the drop-in check; needs the GPU library at run time)
+REF_GPU_SO = os.path.join(HERE, "_ref", "libns3d_ref_gpu.so")
 
 
-def _ref_lib():
-    global _REF
-    if _REF is None:
-        lib = ctypes.CDLL(REF_SO)
+def _ref_lib(path=REF_SO):
+    if path not in _REF:
+        lib = ctypes.CDLL(path)
         D = ctypes.POINTER(ctypes.c_double)
         lib.ref_create.restype = ctypes.c_void_p
         lib.ref_create.argtypes = [ctypes.c_char_p]
@@ -287,15 +292,17 @@ def _ref_lib():
         lib.ref_total_energy.restype = ctypes.c_double
         lib.ref_isotropic_post.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
         lib.ref_init_isotropic.argtypes = [ctypes.c_void_p]
-        _REF = lib
-    return _REF
+        _REF[path] = lib
+    return _REF[path]
 
 
 class Ref:
-    """One single-rank instance of the reference (Field3D + SolverParams)."""
+    """One single-rank instance of the reference (Field3D + SolverParams).
+    `library` selects the build: the reference itself (default) or the
+    reference with the product's shim (REF_GPU_SO)."""
 
-    def __init__(self, cfg: dict):
-        self.lib = _ref_lib()
+    def __init__(self, cfg: dict, library: str = REF_SO):
+        self.lib = _ref_lib(library)
         self.cfg = dict(cfg)
         fd, path = tempfile.mkstemp(suffix=".in")
         with os.fdopen(fd, "w") as f:
