@@ -175,6 +175,31 @@ ns3d_status ns3d_step(ns3d_ctx *ctx, int nsteps);
 /* dt of the last step taken on the device. */
 ns3d_status ns3d_last_dt(ns3d_ctx *ctx, double *dt);
 
+/* ---- allocation-free RHS (no counterpart in the reference) ----------------- */
+
+/* Largest box (nx*ny*nz) ns3d_compute_rhs_noalloc accepts. */
+#define NS3D_NOALLOC_MAX_CELLS 65536
+
+/* compute_rhs for callers that may not allocate device memory: hosts whose
+ * GPU memory is owned by another allocator (a framework's caching allocator,
+ * a fixed per-job budget) or that must not stall on cudaMalloc mid-run. No
+ * context, no cudaMalloc/cudaFree: the caller passes device pointers to the
+ * interior primitives (rho,u,v,w,p; nx*ny*nz each, x fastest) and to `rhs`
+ * (5 consecutive blocks of nx*ny*nz: rho, rhou, rhov, rhow, E), plus the
+ * cudaStream_t to run on (NULL = legacy default stream), on the current
+ * device. The work is enqueued, not waited for. Same result as
+ * ns3d_compute_rhs for the same params (p->precision selects the form).
+ * The intermediates live in one fixed 7.5 MiB array of this library's device
+ * memory, held by every GPU that loads the library until exit; boxes above
+ * NS3D_NOALLOC_MAX_CELLS cells are rejected with NS3D_ERR_INVALID. All calls
+ * share that array and it keeps the last call's contents, so calls that
+ * overlap on the GPU race: serialise them. The first call on each device looks
+ * up the array's device address; make that first call before any stream
+ * capture. */
+ns3d_status ns3d_compute_rhs_noalloc(const ns3d_params *p, const double *rho, const double *u,
+                                     const double *v, const double *w, const double *pres,
+                                     double *rhs, void *stream);
+
 /* ---- instrumentation (no reference counterpart) -------------------------- */
 
 /* Kernel classes timed by ns3d_profile. */

@@ -55,6 +55,8 @@ _SIGS = {
     "ns3d_profile": (_i, [_vp, _i]),
     "ns3d_profile_read": (_i, [_vp, _D, ctypes.POINTER(ctypes.c_longlong)]),
     "ns3d_launch_count": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    # device pointers and the stream passed as integers (c_void_p)
+    "ns3d_compute_rhs_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 

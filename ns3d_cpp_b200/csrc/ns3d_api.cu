@@ -13,6 +13,7 @@
 
 #include "ns3d_gpu.h"
 #define NS3D_API_KERNELS
+#include "ns3d_internal.h"
 #include "ns3d_launch.cuh"
 
 using namespace ns3d;
@@ -457,6 +458,39 @@ ns3d_status compute_sums(ns3d_ctx* ctx, double out[NSUMS]) {
 }
 
 }  // namespace
+
+namespace ns3d {
+
+ns3d_status build_launch_cfg(const ns3d_params* p, LaunchCfg* L, std::string* msg) {
+    if (!p || !L) return NS3D_ERR_INVALID;
+    ns3d_params q = *p;
+    ns3d_status s = ns3d_params_derive(&q);
+    if (s != NS3D_OK) return s;
+    std::string m;
+    if ((s = validate(&q, m)) != NS3D_OK) {
+        if (msg) *msg = m;
+        return s;
+    }
+    std::memset(L, 0, sizeof(*L));
+    DevParams& P = L->P;
+    P.nx = q.global_nx; P.ny = q.global_ny; P.nz = q.global_nz;
+    P.n = (long long)q.global_nx * q.global_ny * q.global_nz;
+    P.gamma = q.gamma; P.Rgas = q.Rgas; P.mu = q.mu; P.Cp = q.Cp; P.Pr = q.Pr;
+    P.sutherland_s = q.sutherland_s_over_tref; P.sw_eps = q.sw_entropy_eps;
+    P.dx = q.dx; P.dy = q.dy; P.dz = q.dz;
+    P.inv_dx = 1.0 / q.dx; P.inv_dy = 1.0 / q.dy; P.inv_dz = 1.0 / q.dz;
+    P.cfl = q.cfl; P.dt_fixed = q.dt_fixed;
+    linear_coefficients(q, P.lin);
+    P.mdcd_disp = q.mdcd_disp; P.mdcd_diss = q.mdcd_diss;
+    P.vis_order = q.vis_scheme == NS3D_VIS_C4TH ? 4 : (q.vis_scheme == NS3D_VIS_C6TH ? 6 : 8);
+    L->fvs = q.fvs_type == NS3D_FVS_STEGER_WARMING ? FV_SW : FV_LF;
+    L->rc = recon_kind(q.recon);
+    for (int d = 0; d < 3; ++d) L->seg[d] = 32;
+    L->stream = nullptr;
+    return NS3D_OK;
+}
+
+}  // namespace ns3d
 
 // ===========================================================================
 // C ABI
