@@ -309,11 +309,13 @@ def our_arm(args, rank, world, local):
 
     # --- the plain FP64 form on the same workload ---
     k64 = max(3, args.steps // 3)
-    with ns.Solver(make_params(ns, n, "fp64"), device=local) as s:
-        s.upload_primitive(W)
-        ms64, _, prof64 = timed_steps(torch, s, k64, max(3, args.warmup // 2), dist, use_cuda)
-    ms64_max = dist_max(dist, ms64, use_cuda)
-    fp64_sps = world * k64 / (ms64_max / 1e3)
+    fp64_sps, ms64_max, prof64 = None, None, {}
+    if not args.skip_fp64:
+        with ns.Solver(make_params(ns, n, "fp64"), device=local) as s:
+            s.upload_primitive(W)
+            ms64, _, prof64 = timed_steps(torch, s, k64, max(3, args.warmup // 2), dist, use_cuda)
+        ms64_max = dist_max(dist, ms64, use_cuda)
+        fp64_sps = world * k64 / (ms64_max / 1e3)
 
     if rank != 0:
         if dist is not None:
@@ -321,7 +323,7 @@ def our_arm(args, rank, world, local):
         return
 
     errors = error_run(ns, n, W, args.err_steps, local) if args.err_steps > 0 else None
-    e2e = e2e_run(torch, ns, n, W, args.e2e_steps, local)
+    e2e = e2e_run(torch, ns, n, W, args.e2e_steps, local) if args.e2e_steps > 0 else None
 
     # dominant kernel roofline (per launch, CUDA-event timed in the timed region)
     rsize = 4
@@ -334,11 +336,15 @@ def our_arm(args, rank, world, local):
                          "alg_bytes_per_launch": b,
                          "achieved_gbs": b / (kms / cnt / 1e3) / 1e9 if b else None}
     dom = max((c for c in kern if c != "other"), key=lambda c: kern[c]["ms_total"])
-    traffic = ncu_traffic().get(f"fp32acc64/{dom}")
+    tr = ncu_traffic()
+    traffic = tr.get(f"fp32acc64/{dom}")
+    traffic = None if traffic is None else traffic * 1e9 * (ncell / 256 ** 3)
     ach = kern[dom]["achieved_gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
-                "alg_bytes_per_cell": kernel_bytes_per_cell(dom, rsize)}
+                "alg_bytes_per_cell": kernel_bytes_per_cell(dom, rsize),
+                "alg_bytes_per_launch": kern[dom]["alg_bytes_per_launch"],
+                "traffic_source": tr.get("source") if traffic is not None else None}
     step_ach = STEP_BYTES_PER_CELL * ncell * (value / world) / 1e9
     roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s",
                      "frac": step_ach / peak, "alg_bytes_per_cell_step": STEP_BYTES_PER_CELL}
@@ -358,11 +364,12 @@ def our_arm(args, rank, world, local):
                    "l2": f"inputs larger than L2: {6 * ncell * 8 / 1e6:.0f} MB per state buffer",
                    "parallelism": f"replicas x{world}"},
         "gcell_per_s": value * ncell / 1e9,
-        "fp64": {"steps_per_s": fp64_sps, "gcell_per_s": fp64_sps * ncell / 1e9,
-                 "steps": k64, "ms_per_step": ms64_max / k64,
-                 "kernels_ms_per_launch": {c: (v[0] / v[1] if v[1] else None)
-                                           for c, v in prof64.items()}},
-        "fp32_over_fp64": value / fp64_sps,
+        "fp64": None if fp64_sps is None else {
+            "steps_per_s": fp64_sps, "gcell_per_s": fp64_sps * ncell / 1e9,
+            "steps": k64, "ms_per_step": ms64_max / k64,
+            "kernels_ms_per_launch": {c: (v[0] / v[1] if v[1] else None)
+                                      for c, v in prof64.items()}},
+        "fp32_over_fp64": None if fp64_sps is None else value / fp64_sps,
         "errors_fp32_vs_fp64": errors,
         "roofline": roofline, "roofline_step": roofline_step, "kernels": kern,
         "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
@@ -471,6 +478,7 @@ def main(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true", help="only the headline form")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     rank, world, local = env_rank()
