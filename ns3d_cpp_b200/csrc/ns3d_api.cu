@@ -485,7 +485,7 @@ ns3d_status build_launch_cfg(const ns3d_params* p, LaunchCfg* L, std::string* ms
     P.vis_order = q.vis_scheme == NS3D_VIS_C4TH ? 4 : (q.vis_scheme == NS3D_VIS_C6TH ? 6 : 8);
     L->fvs = q.fvs_type == NS3D_FVS_STEGER_WARMING ? FV_SW : FV_LF;
     L->rc = recon_kind(q.recon);
-    for (int d = 0; d < 3; ++d) L->seg[d] = 32;
+    for (int d = 0; d < 3; ++d) L->seg[d] = 0;  // chosen per launch from the grid
     L->stream = nullptr;
     return NS3D_OK;
 }
@@ -531,7 +531,7 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
     P.vis_order = q.vis_scheme == NS3D_VIS_C4TH ? 4 : (q.vis_scheme == NS3D_VIS_C6TH ? 6 : 8);
     ctx->L.fvs = q.fvs_type == NS3D_FVS_STEGER_WARMING ? FV_SW : FV_LF;
     ctx->L.rc = recon_kind(q.recon);
-    for (int d = 0; d < 3; ++d) ctx->L.seg[d] = 32;
+    for (int d = 0; d < 3; ++d) ctx->L.seg[d] = 0;  // chosen per launch from the grid
     ctx->rsize = q.precision == NS3D_PREC_FP64 ? sizeof(double) : sizeof(float);
 
     auto bail = [&](ns3d_status st, const std::string& m) {

@@ -115,11 +115,21 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     // face-flux difference. The FP64 form keeps the reference's arithmetic.
     constexpr bool kDeviation = sizeof(R) < sizeof(double);
     double refp[5], refm[5];
-    auto load_split = [&](int s, R* Fp, R* Fm, bool set_ref) {
+    // Loads of one cell's primitives are issued a step before the cell is
+    // split (`load_raw` into registers), so their latency hides behind the
+    // reconstruction of the current face instead of stalling the march.
+    auto load_raw = [&](int s, double* raw) {
         const long long id = base + (long long)wrap1(s, len) * stride;
+        raw[0] = W.rho[id];
+        raw[1] = W.u[id];
+        raw[2] = W.v[id];
+        raw[3] = W.w[id];
+        raw[4] = W.p[id];
+    };
+    auto split_raw = [&](const double* raw, R* Fp, R* Fm, bool set_ref) {
         if constexpr (!kDeviation) {
-            R rr = R(W.rho[id]);
-            const R u = R(W.u[id]), v = R(W.v[id]), w = R(W.w[id]), p = R(W.p[id]);
+            R rr = R(raw[0]);
+            const R u = R(raw[1]), v = R(raw[2]), w = R(raw[3]), p = R(raw[4]);
             if (rr <= R(0)) rr = R(1e-12);
             R E, c;
             p2c_Ec(rr, u, v, w, p, gamma, E, c);
@@ -128,8 +138,8 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
             else
                 split_lf<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fp, Fm);
         } else {
-            double rr = W.rho[id];
-            const double u = W.u[id], v = W.v[id], w = W.w[id], p = W.p[id];
+            double rr = raw[0];
+            const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
             if (rr <= 0.0) rr = 1e-12;
             double E, c, Fpd[5], Fmd[5];
             p2c_Ec<double>(rr, u, v, w, p, P.gamma, E, c);
@@ -156,11 +166,29 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     (void)eps;
 
     int f = c0 - 1;  // face f sits between cells f and f+1 (the reference's i_face = f + ng)
+    double nxt[5];
 #pragma unroll
-    for (int m = 0; m < S - 1; ++m) load_split(f - MID + m, fp[m], fm[m], m == 0);
+    for (int m = 0; m < S - 1; ++m) {
+        load_raw(f - MID + m, nxt);
+        split_raw(nxt, fp[m], fm[m], m == 0);
+    }
+    load_raw(f - MID + S - 1, nxt);
     R prev[5];
     for (int t = 0; f < c1; ++t, ++f) {
-        load_split(f - MID + S - 1, fp[S - 1], fm[S - 1], S == 1);
+        double cur[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) cur[q] = nxt[q];
+        // the following cell (in range by wrap-around even past the segment end)
+        load_raw(f - MID + S, nxt);
+        R old[5];
+        const long long oid = base + (long long)f * stride;
+        if constexpr (DIR != 0) {
+            if (t > 0) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) old[q] = tacc[q * n + oid];
+            }
+        }
+        split_raw(cur, fp[S - 1], fm[S - 1], false);
         R face[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -175,14 +203,13 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
             face[q] = plus_face + minus_face;
         }
         if (t > 0) {
-            const long long id = base + (long long)f * stride;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 const R d = face[q] - prev[q];
                 if constexpr (DIR == 0)
-                    tacc[q * n + id] = d * inv_h;
+                    tacc[q * n + oid] = d * inv_h;
                 else
-                    tacc[q * n + id] = tacc[q * n + id] + d * inv_h;
+                    tacc[q * n + oid] = old[q] + d * inv_h;
             }
         }
 #pragma unroll
@@ -194,6 +221,175 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
                 fp[m][q] = fp[m + 1][q];
                 fm[m][q] = fm[m + 1][q];
             }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x sweep, warp per periodic row (nx a multiple of 32). Lanes hold 32
+// consecutive cells, so loads and stores are coalesced; the split fluxes of
+// the previous, current and next 32-cell chunks live in a per-warp shared
+// ring, and every lane reconstructs one face per chunk. The face on the -x
+// side of a lane's cell comes from the neighbouring lane (shuffle). Each cell
+// of the row is split exactly once: the last and first chunks, needed twice by
+// periodicity, are kept in registers. Same arithmetic per face and cell as
+// k_sweep<0> (the FP64 results are identical); in the FP32-stencil form the
+// split-flux offset is the row's first cell.
+// ---------------------------------------------------------------------------
+constexpr int XW_WARPS = 4;
+
+template <class R, int FVS, int RC>
+__global__ void __launch_bounds__(32 * XW_WARPS)
+k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
+    if (ctrl && ctrl->stop) return;
+    constexpr int S = Stencil<RC>::S;
+    constexpr int MID = (S - 1) / 2;
+    constexpr bool kDeviation = sizeof(R) < sizeof(double);
+    __shared__ R ring[XW_WARPS][2][5][96];  // [warp][+/-][component][3 chunks x 32]
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int nx = P.nx;
+    const long long n = P.n;
+    const long long row = (long long)blockIdx.x * XW_WARPS + wq;
+    if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
+    const long long base = row * nx;
+    const int nch = nx >> 5;
+    const R gamma = R(P.gamma), eps = R(P.sw_eps);
+    R lin[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) lin[m] = R(P.lin[m]);
+    const R disp = R(P.mdcd_disp), diss = R(P.mdcd_diss);
+    const R inv_h = R(P.inv_dx);
+    (void)gamma;
+    (void)eps;
+
+    double refp[5], refm[5];
+    auto load_raw = [&](int chunk, double* raw) {
+        const long long id = base + (chunk << 5) + lane;
+        raw[0] = W.rho[id];
+        raw[1] = W.u[id];
+        raw[2] = W.v[id];
+        raw[3] = W.w[id];
+        raw[4] = W.p[id];
+    };
+    auto split_raw = [&](const double* raw, R* Fp, R* Fm) {
+        if constexpr (!kDeviation) {
+            R rr = R(raw[0]);
+            const R u = R(raw[1]), v = R(raw[2]), w = R(raw[3]), p = R(raw[4]);
+            if (rr <= R(0)) rr = R(1e-12);
+            R E, c;
+            p2c_Ec(rr, u, v, w, p, gamma, E, c);
+            if constexpr (FVS == FV_SW) split_sw<R, 1, 0, 0>(rr, u, v, w, E, p, c, gamma, eps, Fp, Fm);
+            else split_lf<R, 1, 0, 0>(rr, u, v, w, E, p, c, Fp, Fm);
+        } else {
+            double rr = raw[0];
+            const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
+            if (rr <= 0.0) rr = 1e-12;
+            double E, c, Fpd[5], Fmd[5];
+            p2c_Ec<double>(rr, u, v, w, p, P.gamma, E, c);
+            if constexpr (FVS == FV_SW)
+                split_sw<double, 1, 0, 0>(rr, u, v, w, E, p, c, P.gamma, P.sw_eps, Fpd, Fmd);
+            else
+                split_lf<double, 1, 0, 0>(rr, u, v, w, E, p, c, Fpd, Fmd);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                Fp[q] = R(Fpd[q] - refp[q]);
+                Fm[q] = R(Fmd[q] - refm[q]);
+            }
+        }
+    };
+    // the FP32 form's offset: the split flux of the row's first cell
+    if constexpr (kDeviation) {
+        double raw[5];
+        load_raw(0, raw);
+        double rr = raw[0];
+        if (rr <= 0.0) rr = 1e-12;
+        double E, c, Fpd[5], Fmd[5];
+        p2c_Ec<double>(rr, raw[1], raw[2], raw[3], raw[4], P.gamma, E, c);
+        if constexpr (FVS == FV_SW)
+            split_sw<double, 1, 0, 0>(rr, raw[1], raw[2], raw[3], E, raw[4], c, P.gamma, P.sw_eps, Fpd, Fmd);
+        else
+            split_lf<double, 1, 0, 0>(rr, raw[1], raw[2], raw[3], E, raw[4], c, Fpd, Fmd);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            refp[q] = __shfl_sync(0xffffffffu, Fpd[q], 0);
+            refm[q] = __shfl_sync(0xffffffffu, Fmd[q], 0);
+        }
+    }
+    R (*rp)[96] = ring[wq][0];
+    R (*rm)[96] = ring[wq][1];
+    auto put = [&](int slot, const R* Fp, const R* Fm) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            rp[q][slot * 32 + lane] = Fp[q];
+            rm[q][slot * 32 + lane] = Fm[q];
+        }
+    };
+    // face at chunk-relative position `pos` (face pos sits between cells pos and
+    // pos+1 of the chunk in slot `cs`); window cells pos-MID .. pos-MID+S-1
+    auto face_at = [&](int cs, int pos, R* face) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            R a[S], b[S];
+#pragma unroll
+            for (int m = 0; m < S; ++m) {
+                int k = cs * 32 + pos - MID + m;
+                k = k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
+                a[m] = rp[q][k];
+            }
+#pragma unroll
+            for (int m = 0; m < S; ++m) {
+                int k = cs * 32 + pos - MID + (S - 1 - m);
+                k = k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
+                b[m] = rm[q][k];
+            }
+            const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+            const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+            face[q] = plus_face + minus_face;
+        }
+    };
+
+    // prologue: slot 0 <- last chunk, slot 1 <- chunk 0
+    R lastp[5], lastm[5], firstp[5], firstm[5];
+    double raw[5], nxt[5];
+    load_raw(nch - 1, raw);
+    split_raw(raw, lastp, lastm);
+    load_raw(0, raw);
+    split_raw(raw, firstp, firstm);
+    put(0, lastp, lastm);
+    put(1, firstp, firstm);
+    if (nch > 1) load_raw(1, nxt);
+    __syncwarp();
+    // the face on the -x side of cell 0 (face nx-1 by periodicity)
+    R carry[5];
+    face_at(1, -1, carry);
+    int cur = 1;
+    for (int c = 0; c < nch; ++c) {
+        const int nslot = cur == 2 ? 0 : cur + 1;
+        R Fp[5], Fm[5];
+        if (c + 1 == nch) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { Fp[q] = firstp[q]; Fm[q] = firstm[q]; }
+        } else if (c + 2 == nch) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { Fp[q] = lastp[q]; Fm[q] = lastm[q]; }
+        } else {
+            split_raw(nxt, Fp, Fm);
+        }
+        __syncwarp();
+        put(nslot, Fp, Fm);
+        if (c + 2 < nch - 1) load_raw(c + 2, nxt);
+        const long long id = base + (c << 5) + lane;
+        __syncwarp();
+        R face[5];
+        face_at(cur, lane, face);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            R left = __shfl_up_sync(0xffffffffu, face[q], 1);
+            if (lane == 0) left = carry[q];
+            carry[q] = __shfl_sync(0xffffffffu, face[q], 31);
+            const R d = face[q] - left;
+            tacc[q * n + id] = d * inv_h;
+        }
+        cur = nslot;
     }
 }
 

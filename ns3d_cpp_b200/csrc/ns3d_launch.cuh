@@ -34,13 +34,31 @@ namespace detail {
 
 inline int threads_for(int ext) { return ext >= 128 ? 128 : (ext >= 64 ? 64 : 32); }
 
+// Cells per marching segment: long segments amortise the S-1 halo splits at
+// the segment start, short ones give enough threads to fill 148 SMs. Aim for
+// about two waves of 16 warps per SM, within [16, 64] cells (and <= len).
+inline int segment_for(int len, long long lines) {
+    const long long target = 148LL * 512 * 2;
+    long long nseg = (target + lines - 1) / lines;
+    int seg = (int)((len + nseg - 1) / nseg);
+    seg = (seg + 7) / 8 * 8;
+    seg = seg < 16 ? 16 : (seg > 64 ? 64 : seg);
+    return seg > len ? len : seg;
+}
+
 template <int DIR, class R, int FVS, int RC>
 cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl) {
     const DevParams& P = L.P;
+    if (DIR == 0 && P.nx % 32 == 0) {
+        const long long rows = (long long)P.ny * P.nz;
+        const unsigned blocks = (unsigned)((rows + XW_WARPS - 1) / XW_WARPS);
+        k_sweep_x_warp<R, FVS, RC><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
+        return cudaGetLastError();
+    }
     const int ext = DIR == 0 ? P.ny : P.nx;        // thread dimension
     const int other = DIR == 2 ? P.ny : P.nz;     // blockIdx.y dimension
     const int len = DIR == 0 ? P.nx : (DIR == 1 ? P.ny : P.nz);
-    const int seg = L.seg[DIR] > 0 ? L.seg[DIR] : len;
+    const int seg = L.seg[DIR] > 0 ? L.seg[DIR] : segment_for(len, (long long)ext * other);
     const int th = threads_for(ext);
     dim3 grid((ext + th - 1) / th, other, (len + seg - 1) / seg);
     k_sweep<DIR, R, FVS, RC><<<grid, th, 0, L.stream>>>(P, W, tacc, seg, ctrl);
