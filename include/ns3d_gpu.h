@@ -175,6 +175,31 @@ ns3d_status ns3d_step(ns3d_ctx *ctx, int nsteps);
 /* dt of the last step taken on the device. */
 ns3d_status ns3d_last_dt(ns3d_ctx *ctx, double *dt);
 
+/* ---- discrete adjoint (no counterpart in the reference) ------------------- */
+/* The derivative of exactly the FP64 forward arithmetic (the adjoint of the
+ * discretisation, not of the PDE). Supported: FP64 form, Steger-Warming (use
+ * sw_entropy_eps > 0 to make |lambda| smooth) or Lax-Friedrichs, WENO5 or the
+ * linear reconstructions; MDCD_HYBRID returns NS3D_ERR_UNSUPPORTED. Arrays
+ * are host pointers to 5 consecutive interior blocks (rho, u, v, w, p). */
+
+/* lam_w = (d rhs / d w)^T lam_rhs at the current state (vector-Jacobian
+ * product of compute_rhs with respect to the primitives). */
+ns3d_status ns3d_rhs_vjp(ns3d_ctx *ctx, const double *lam_rhs, double *lam_w);
+/* `nsteps` runge_kutta_3 steps with the given dt sequence (each step records
+ * U0 first, as time_advance does). */
+ns3d_status ns3d_step_dts(ns3d_ctx *ctx, int nsteps, const double *dts);
+/* Gradient of an end-time objective with respect to the current state,
+ * through `nsteps` RK3 steps. dts: the dt of every step (NULL: the CFL dt of
+ * each step, written to dts_out when that is non-NULL); dt is held fixed, not
+ * differentiated. lam_final: dJ/dw at the end state, or NULL for J = the total
+ * kinetic energy sum 0.5 rho |u|^2 dV of compute_total_energy
+ * (postprocess.cpp:103), whose value is returned in *J. grad receives dJ/dw
+ * at the start state. The forward run stores the state every
+ * `checkpoint_every` steps; the reverse sweep recomputes each segment's stage
+ * states from its checkpoint. Afterwards the context holds the end state. */
+ns3d_status ns3d_adjoint(ns3d_ctx *ctx, int nsteps, int checkpoint_every, const double *dts,
+                         double *dts_out, const double *lam_final, double *grad, double *J);
+
 /* ---- allocation-free RHS (no counterpart in the reference) ----------------- */
 
 /* Largest box (nx*ny*nz) ns3d_compute_rhs_noalloc accepts. */

@@ -55,6 +55,9 @@ _SIGS = {
     "ns3d_profile": (_i, [_vp, _i]),
     "ns3d_profile_read": (_i, [_vp, _D, ctypes.POINTER(ctypes.c_longlong)]),
     "ns3d_launch_count": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "ns3d_rhs_vjp": (_i, [_vp, _D, _D]),
+    "ns3d_step_dts": (_i, [_vp, _i, _D]),
+    "ns3d_adjoint": (_i, [_vp, _i, _i, _D, _D, _D, _D, _D]),
     # device pointers and the stream passed as integers (c_void_p)
     "ns3d_compute_rhs_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }

@@ -46,6 +46,7 @@ UNITS = {
     "ns3d_fp32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "ns3d_api.cu": ["--fmad=false"],
     "ns3d_noalloc.cu": ["--fmad=false"],
+    "ns3d_adjoint.cu": ["--fmad=true"],
     "ns3d_params.cpp": [],
 }
 

@@ -326,6 +326,24 @@ ns3d_status update_t(ns3d_ctx* ctx, int stage, StateView Wc, StateView W0, int b
     return NS3D_OK;
 }
 
+// A stage on explicit state arrays (6 blocks of n each); FP64 form.
+StateView view_at(double* base, long long n) {
+    return StateView{base, base + n, base + 2 * n, base + 3 * n, base + 4 * n, base + 5 * n};
+}
+StateOut out_at(double* base, long long n) {
+    return StateOut{base, base + n, base + 2 * n, base + 3 * n, base + 4 * n, base + 5 * n};
+}
+
+ns3d_status stage_at(ns3d_ctx* ctx, int stage, double* wc, double* w0, double* wn) {
+    const StateView Wc = view_at(wc, ctx->n), W0 = view_at(w0, ctx->n);
+    ns3d_status s = launch_rhs_parts(ctx, Wc, ctx->ctrl);
+    if (s != NS3D_OK) return s;
+    NS3D_LAUNCH(NS3D_KERNEL_UPDATE, 1,
+                launch_update<double>(ctx->L, stage, Wc, W0, (const double*)ctx->tacc,
+                                      (const double*)ctx->fv, out_at(wn, ctx->n), ctx->ctrl));
+    return NS3D_OK;
+}
+
 ns3d_status launch_stage(ns3d_ctx* ctx, int stage, int bc, int b0, int bn) {
     const StateView Wc = view(ctx, bc), W0 = view(ctx, b0);
     ns3d_status s = launch_rhs_parts(ctx, Wc, ctx->ctrl);
@@ -840,6 +858,155 @@ ns3d_status ns3d_energy_spectrum(ns3d_ctx* ctx, double* Ek, int nbins) {
         NS3D_CK(cudaGetLastError());
     }
     NS3D_CK(cudaMemcpyAsync(Ek, ctx->bins, sizeof(double) * nbins, cudaMemcpyDeviceToHost, ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+// ---- discrete adjoint -------------------------------------------------------
+
+namespace {
+
+// Device scratch of one adjoint call, released when it goes out of scope.
+struct DevBuf {
+    double* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    bool alloc(size_t count) { return cudaMalloc(&p, sizeof(double) * count) == cudaSuccess; }
+};
+
+ns3d_status adjoint_supported(ns3d_ctx* ctx) {
+    if (ctx->p.precision != NS3D_PREC_FP64)
+        return fail(ctx, NS3D_ERR_UNSUPPORTED, "the adjoint differentiates the FP64 form");
+    if (ctx->L.rc == RC_MDCD_HYBRID)
+        return fail(ctx, NS3D_ERR_UNSUPPORTED, "no adjoint for MDCD_HYBRID");
+    return NS3D_OK;
+}
+
+ns3d_status set_dt(ns3d_ctx* ctx, double dt) {
+    NS3D_CK(cudaMemcpyAsync(&ctx->ctrl->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    // a pageable source: the copy has been staged when cudaMemcpyAsync returns
+    return NS3D_OK;
+}
+
+}  // namespace
+
+ns3d_status ns3d_rhs_vjp(ns3d_ctx* ctx, const double* lam_rhs, double* lam_w) {
+    if (!ctx || !lam_rhs || !lam_w) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    ns3d_status s = adjoint_supported(ctx);
+    if (s != NS3D_OK) return s;
+    const long long n = ctx->n;
+    DevBuf lr, lw, G, lg;
+    if (!lr.alloc(5 * n) || !lw.alloc(5 * n) || !G.alloc((size_t)adj_scratch_blocks(ctx->L) * n) ||
+        !lg.alloc(16 * n))
+        return fail(ctx, NS3D_ERR_NOMEM, "adjoint scratch allocation failed");
+    NS3D_CK(cudaMemcpyAsync(lr.p, lam_rhs, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, ctx->stream));
+    NS3D_CK(cudaMemsetAsync(lw.p, 0, sizeof(double) * 5 * n, ctx->stream));
+    NS3D_LAUNCH(NS3D_KERNEL_OTHER, 11, adj_rhs_vjp(ctx->L, view(ctx, ctx->cur), lr.p, G.p, lg.p, lw.p));
+    NS3D_CK(cudaMemcpyAsync(lam_w, lw.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_step_dts(ns3d_ctx* ctx, int nsteps, const double* dts) {
+    if (!ctx || nsteps < 0 || (nsteps > 0 && !dts)) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    ns3d_status s = reset_ctrl(ctx);
+    if (s != NS3D_OK) return s;
+    for (int k = 0; k < nsteps; ++k) {
+        ctx->rec = ctx->cur;
+        if ((s = set_dt(ctx, dts[k])) != NS3D_OK) return s;
+        if ((s = enqueue_rk3(ctx)) != NS3D_OK) return s;
+    }
+    ctx->dtmin_valid = false;
+    if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
+    if (ctx->ctrl_host->bad_cell < ctx->n) return fail(ctx, NS3D_ERR_NONPHYSICAL, "non-physical state");
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_adjoint(ns3d_ctx* ctx, int nsteps, int K, const double* dts_in, double* dts_out,
+                         const double* lam_final, double* grad, double* J) {
+    if (!ctx || nsteps < 1 || K < 1 || !grad) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    ns3d_status s = adjoint_supported(ctx);
+    if (s != NS3D_OK) return s;
+    const long long n = ctx->n;
+    const size_t st = 6 * (size_t)n;  // one state: rho,u,v,w,p,T
+    const int nseg = (nsteps + K - 1) / K;
+    DevBuf ck, ws, la, lb, lu0, lr, G, lg, dtd;
+    if (!ck.alloc(st * nseg) || !ws.alloc(st * (3 * (size_t)K + 1)) || !la.alloc(5 * n) ||
+        !lb.alloc(5 * n) || !lu0.alloc(5 * n) || !lr.alloc(5 * n) ||
+        !G.alloc((size_t)adj_scratch_blocks(ctx->L) * n) || !lg.alloc(16 * n) ||
+        !dtd.alloc(nsteps))
+        return fail(ctx, NS3D_ERR_NOMEM, "adjoint checkpoint/scratch allocation failed");
+    std::vector<double> dts(nsteps);
+
+    // ---- forward run, a checkpoint every K steps, dt recorded ----
+    if ((s = reset_ctrl(ctx)) != NS3D_OK) return s;
+    for (int k = 0; k < nsteps; ++k) {
+        if (k % K == 0)
+            NS3D_CK(cudaMemcpyAsync(ck.p + (size_t)(k / K) * st, warr(ctx, ctx->cur, 0),
+                                    sizeof(double) * st, cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->rec = ctx->cur;
+        if (dts_in) {
+            if ((s = set_dt(ctx, dts_in[k])) != NS3D_OK) return s;
+        } else {
+            std::memcpy(&ctx->ctrl_host->dtmin_bits, &CFL_INIT, sizeof(double));
+            NS3D_CK(cudaMemcpyAsync(&ctx->ctrl->dtmin_bits, &ctx->ctrl_host->dtmin_bits,
+                                    sizeof(unsigned long long), cudaMemcpyHostToDevice, ctx->stream));
+            if ((s = enqueue_cfl(ctx)) != NS3D_OK) return s;
+            NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                        (k_control_pre<<<1, 1, 0, ctx->stream>>>(ctx->ctrl, 0, ctx->p.cfl,
+                                                                  ctx->p.dt_fixed, 0.0, 0.0)));
+        }
+        NS3D_CK(cudaMemcpyAsync(dtd.p + k, &ctx->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+        if ((s = enqueue_rk3(ctx)) != NS3D_OK) return s;
+    }
+    NS3D_CK(cudaMemcpyAsync(dts.data(), dtd.p, sizeof(double) * nsteps, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
+    if (ctx->ctrl_host->bad_cell < n) return fail(ctx, NS3D_ERR_NONPHYSICAL, "non-physical state");
+    ctx->dtmin_valid = false;
+    if (dts_out) std::memcpy(dts_out, dts.data(), sizeof(double) * nsteps);
+    double sums[NSUMS];
+    if ((s = compute_sums(ctx, sums)) != NS3D_OK) return s;
+    if (J) *J = sums[0] * (ctx->p.dx * ctx->p.dy * ctx->p.dz);
+
+    // ---- seed: dJ/dw at the end state ----
+    double* A = la.p;
+    double* B = lb.p;
+    if (lam_final)
+        NS3D_CK(cudaMemcpyAsync(A, lam_final, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, ctx->stream));
+    else
+        NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
+                    adj_seed_ke(ctx->L, view(ctx, ctx->cur), A, ctx->p.dx * ctx->p.dy * ctx->p.dz));
+
+    // ---- reverse sweep, segment by segment ----
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int s0 = seg * K, m = std::min(K, nsteps - s0);
+        NS3D_CK(cudaMemcpyAsync(ws.p, ck.p + (size_t)seg * st, sizeof(double) * st,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+        for (int j = 0; j < m; ++j) {  // recompute the segment's stage states
+            double* w0 = ws.p + (size_t)(3 * j) * st;
+            if ((s = set_dt(ctx, dts[s0 + j])) != NS3D_OK) return s;
+            if ((s = stage_at(ctx, 1, w0, w0, w0 + st)) != NS3D_OK) return s;
+            if ((s = stage_at(ctx, 2, w0 + st, w0, w0 + 2 * st)) != NS3D_OK) return s;
+            if ((s = stage_at(ctx, 3, w0 + 2 * st, w0, w0 + 3 * st)) != NS3D_OK) return s;
+        }
+        for (int j = m - 1; j >= 0; --j) {  // A: adjoint of the step's end state
+            double* w0 = ws.p + (size_t)(3 * j) * st;
+            const double dt = dts[s0 + j];
+            for (int stg = 3; stg >= 1; --stg) {
+                const StateView Wk = view_at(w0 + (size_t)stg * st, n);
+                const StateView Wp = view_at(w0 + (size_t)(stg - 1) * st, n);
+                NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1, adj_stage(ctx->L, stg, Wk, Wp, A, lu0.p, lr.p, B, dt));
+                NS3D_LAUNCH(NS3D_KERNEL_OTHER, 11, adj_rhs_vjp(ctx->L, Wp, lr.p, G.p, lg.p, B));
+                std::swap(A, B);
+            }
+            NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1, adj_finish(ctx->L, view_at(w0, n), lu0.p, A));
+        }
+    }
+    NS3D_CK(cudaMemcpyAsync(grad, A, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->stream));
     NS3D_CK(cudaStreamSynchronize(ctx->stream));
     return NS3D_OK;
 }

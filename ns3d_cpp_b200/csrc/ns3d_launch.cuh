@@ -28,11 +28,11 @@ cudaError_t launch_update(const LaunchCfg& L, int stage, StateView Wc, StateView
 template <class R>
 cudaError_t launch_rhs_out(const LaunchCfg& L, const R* tacc, const R* fv, double* rhs);
 
-#ifdef NS3D_LAUNCH_IMPL
-
 namespace detail {
 
 inline int threads_for(int ext) { return ext >= 128 ? 128 : (ext >= 64 ? 64 : 32); }
+
+inline dim3 cell_grid(const DevParams& P, int th) { return dim3((P.nx + th - 1) / th, P.ny, P.nz); }
 
 // Cells per marching segment: long segments amortise the S-1 halo splits at
 // the segment start, short ones give enough threads to fill 148 SMs. Aim for
@@ -45,6 +45,12 @@ inline int segment_for(int len, long long lines) {
     seg = seg < 16 ? 16 : (seg > 64 ? 64 : seg);
     return seg > len ? len : seg;
 }
+
+}  // namespace detail
+
+#ifdef NS3D_LAUNCH_IMPL
+
+namespace detail {
 
 template <int DIR, class R, int FVS, int RC>
 cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl) {
@@ -83,8 +89,6 @@ cudaError_t sweeps_rc(const LaunchCfg& L, int dir, StateView W, R* tacc, const C
     default: return cudaErrorInvalidValue;
     }
 }
-
-inline dim3 cell_grid(const DevParams& P, int th) { return dim3((P.nx + th - 1) / th, P.ny, P.nz); }
 
 }  // namespace detail
 

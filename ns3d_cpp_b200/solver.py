@@ -246,6 +246,36 @@ class Solver:
         self._ck(self.lib.ns3d_device_bytes(self.ctx, ctypes.byref(b)))
         return b.value
 
+    # -- discrete adjoint ---------------------------------------------------
+    def rhs_vjp(self, lam_rhs):
+        """(d rhs / d W)^T lam_rhs at the current state; both (5, nz, ny, nx)."""
+        lr = np.ascontiguousarray(lam_rhs, dtype=np.float64)
+        if lr.shape != (5,) + self.shape:
+            raise ValueError(f"lam_rhs of shape {lr.shape}")
+        out = np.empty_like(lr)
+        self._ck(self.lib.ns3d_rhs_vjp(self.ctx, _dptr(lr), _dptr(out)))
+        return out
+
+    def step_dts(self, dts) -> None:
+        """runge_kutta_3 steps with a prescribed dt sequence."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        self._ck(self.lib.ns3d_step_dts(self.ctx, len(d), _dptr(d)))
+
+    def adjoint(self, nsteps: int, checkpoint_every: int, dts=None, lam_final=None):
+        """Gradient of an end-time objective w.r.t. the current state.
+        Returns (grad (5, nz, ny, nx), J, dts); J is the total kinetic energy
+        when `lam_final` is None."""
+        grad = np.empty((5,) + self.shape)
+        J = ctypes.c_double(np.nan)
+        dts_out = np.empty(nsteps)
+        din = None if dts is None else np.ascontiguousarray(dts, dtype=np.float64)
+        lf = None if lam_final is None else np.ascontiguousarray(lam_final, dtype=np.float64)
+        self._ck(self.lib.ns3d_adjoint(self.ctx, int(nsteps), int(checkpoint_every),
+                                       None if din is None else _dptr(din), _dptr(dts_out),
+                                       None if lf is None else _dptr(lf), _dptr(grad),
+                                       ctypes.byref(J)))
+        return grad, J.value, (dts_out if din is None else din)
+
     # -- instrumentation ----------------------------------------------------
     KERNEL_CLASSES = ("sweep_x", "sweep_y", "sweep_z", "visc_flux", "update", "other")
 
