@@ -15,7 +15,12 @@ struct LaunchCfg {
     int rc;       // RC_* of the reconstruction
     int seg[3];   // cells per thread segment along x, y, z
     cudaStream_t stream;
+    int zb;       // planes per block of the 2.5-D viscous kernels
+    int tiled;    // bit 0: 2.5-D visc_flux, bit 1: 2.5-D update (when the box tiles)
 };
+
+// Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED for tuning.
+void default_tiling(LaunchCfg& L);
 
 // One inviscid sweep (dir 0, 1, 2 in this order per RHS evaluation).
 template <class R>
@@ -98,8 +103,26 @@ cudaError_t launch_sweep(const LaunchCfg& L, int dir, StateView W, R* tacc, cons
                           : detail::sweeps_rc<R, FV_LF>(L, dir, W, tacc, ctrl);
 }
 
+namespace detail {
+inline bool tiles_25d(const LaunchCfg& L, int bit) {
+    return (L.tiled & bit) && L.zb > 0 && L.P.nx % VT_X == 0 && L.P.ny % VT_Y == 0;
+}
+inline dim3 grid_25d(const LaunchCfg& L) {
+    return dim3(L.P.nx / VT_X, L.P.ny / VT_Y, (L.P.nz + L.zb - 1) / L.zb);
+}
+}  // namespace detail
+
 template <class R>
 cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl) {
+    if (detail::tiles_25d(L, 1)) {
+        const dim3 g = detail::grid_25d(L), b(VT_X, VT_Y);
+        switch (L.P.vis_order) {
+        case 4: k_visc_flux_25d<R, 4><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, L.zb); break;
+        case 6: k_visc_flux_25d<R, 6><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, L.zb); break;
+        default: k_visc_flux_25d<R, 8><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, L.zb); break;
+        }
+        return cudaGetLastError();
+    }
     const int th = detail::threads_for(L.P.nx);
     const dim3 g = detail::cell_grid(L.P, th);
     switch (L.P.vis_order) {
@@ -113,6 +136,13 @@ cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl*
 template <class R, int ORD>
 static cudaError_t update_ord(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
                               const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl) {
+    if (detail::tiles_25d(L, 2)) {
+        const dim3 g = detail::grid_25d(L), b(VT_X, VT_Y);
+        if (stage == 1) k_update_25d<R, ORD, 1><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, L.zb);
+        else if (stage == 2) k_update_25d<R, ORD, 2><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, L.zb);
+        else k_update_25d<R, ORD, 3><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, L.zb);
+        return cudaGetLastError();
+    }
     const int th = detail::threads_for(L.P.nx);
     const dim3 g = detail::cell_grid(L.P, th);
     if (stage == 1) k_update<R, ORD, 1><<<g, th, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl);
