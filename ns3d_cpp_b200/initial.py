@@ -60,22 +60,43 @@ def solenoidal_field(n: int, k0: float = 4.0, seed: int = 12345) -> np.ndarray:
     (3, n, n, n) with unit-free amplitude; callers rescale.
     """
     rng = np.random.default_rng(seed)
-    k = np.fft.fftfreq(n, 1.0 / n)
-    K3, K2, K1 = np.meshgrid(k, k, k, indexing="ij")
+    phases = 2.0 * math.pi * rng.random((3, n, n, n))   # the one random draw
+    try:
+        import torch
+        use_gpu = n >= 128 and torch.cuda.is_available()
+    except Exception:  # torch is optional here
+        use_gpu = False
+    if use_gpu:
+        xp = torch
+        dev = "cuda"
+        a = torch.from_numpy(phases).to(dev)
+        k = torch.fft.fftfreq(n, 1.0 / n, dtype=torch.float64, device=dev)
+    else:
+        xp = np
+        a = phases
+        k = np.fft.fftfreq(n, 1.0 / n)
+    K1 = k.reshape(1, 1, n)
+    K2 = k.reshape(1, n, 1)
+    K3 = k.reshape(n, 1, 1)
     kk = K1 * K1 + K2 * K2 + K3 * K3
-    kk_safe = np.where(kk == 0, 1.0, kk)
-    Ak = math.sqrt(2.0 / 3.0) * np.sqrt(kk * np.exp(-2.0 * kk / (k0 * k0)) / (4.0 * math.pi))
-    a = 2.0 * math.pi * rng.random((3,) + kk.shape)
-    vr = Ak * np.sin(a)
-    vi = Ak * np.cos(a)
+    kk_safe = xp.where(kk == 0, xp.ones_like(kk), kk)
+    Ak = math.sqrt(2.0 / 3.0) * xp.sqrt(kk * xp.exp(-2.0 * kk / (k0 * k0)) / (4.0 * math.pi))
+    vr = Ak * xp.sin(a)
+    vi = Ak * xp.cos(a)
+    del a
     vkr = K1 * vr[0] + K2 * vr[1] + K3 * vr[2]
     vki = K1 * vi[0] + K2 * vi[1] + K3 * vi[2]
     out = np.empty((3, n, n, n))
     for c, Kc in enumerate((K1, K2, K3)):
         re = Kc * vkr / kk_safe - vr[c]
         im = Kc * vki / kk_safe - vi[c]
-        spec = np.where(kk == 0, 0.0, re + 1j * im)
-        out[c] = np.fft.ifftn(spec).real
+        zero = kk == 0
+        if use_gpu:
+            spec = torch.complex(torch.where(zero, 0.0, re), torch.where(zero, 0.0, im))
+            out[c] = torch.fft.ifftn(spec).real.cpu().numpy()
+        else:
+            spec = np.where(zero, 0.0, re + 1j * im)
+            out[c] = np.fft.ifftn(spec).real
     return out
 
 

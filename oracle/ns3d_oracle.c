@@ -46,6 +46,8 @@ typedef struct orc_params {
     double sutherland_s;         /* S/Tref; 110.4/288.15 as field_structures.h:100 */
     int nx, ny, nz;
     int fvs, recon, vis;
+    int mu_variant;              /* 0: pow(T, 1.5) as the reference; 1: T*sqrt(T) (a
+                                    1-ulp perturbation, for sensitivity controls) */
 } orc_params;
 
 #define IDX(i, j, k) (((long)(k) * ny + (j)) * nx + (i))
@@ -59,7 +61,8 @@ static inline int wrap(int i, int n) { i %= n; return i < 0 ? i + n : i; }
 /* SolverParams::get_mu, field_structures.h:94-105 (Sutherland). */
 static inline double get_mu(const orc_params *P, double T) {
     double S_ref = P->sutherland_s;
-    return P->mu * pow(T, 1.5) * (1.0 + S_ref) / (T + S_ref);
+    double t15 = P->mu_variant ? T * sqrt(T) : pow(T, 1.5);
+    return P->mu * t15 * (1.0 + S_ref) / (T + S_ref);
 }
 
 /* primitiveToConserved, field_structures.h:430-451 (one cell). */

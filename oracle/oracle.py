@@ -95,7 +95,7 @@ class OrcParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ("gamma", "Pr", "Ma", "Re", "Cv", "Cp", "Rgas", "mu", "dx", "dy", "dz",
                  "mdcd_diss", "mdcd_disp", "ud7l_alpha", "sw_eps", "sutherland_s")] + \
-              [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "fvs", "recon", "vis")]
+              [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "fvs", "recon", "vis", "mu_variant")]
 
 
 def _dp(a: np.ndarray):
@@ -140,6 +140,7 @@ class Oracle:
         self.cfg = dict(cfg)
         d = derived(cfg)
         self.d = d
+        d.setdefault("mu_variant", int(cfg.get("mu_variant", 0)))
         self.p = OrcParams(**{f: d[f] for f, _ in OrcParams._fields_})
         self.shape = (d["nz"], d["ny"], d["nx"])
         self.lib = _orc_lib()
