@@ -482,8 +482,14 @@ __global__ void __launch_bounds__(VT_X * VT_Y)
 k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict__ ctrl,
                 int zb) {
     if (ctrl && ctrl->stop) return;
+    // FP32-stencil form: values enter the tile and the z queue as float
+    // deviations from one reference per block and variable (formed in
+    // double), so each value is converted once; central stencils' weights sum
+    // to zero, so the reference drops out of every derivative. FP64 form: the
+    // reference is 0 and x - 0.0 == x, the reference's arithmetic unchanged.
     constexpr bool kDeviation = sizeof(R) < sizeof(double);
-    __shared__ double tile[4][VT_SY][VT_SX];
+    using TT = R;
+    __shared__ TT tile[4][VT_SY][VT_SX];
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const long long n = P.n, sxy = (long long)nx * ny;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * VT_X + tx;
@@ -491,13 +497,17 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
     const int i = i0 + tx, j = j0 + ty;
     const int k0 = blockIdx.z * zb, k1 = min(k0 + zb, nz);
     const double* src[4] = {W.u, W.v, W.w, W.T};
-    double q[4][9];  // z queue: q[v][m] = value at k - 4 + m
+    double ref[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+        ref[v] = kDeviation ? src[v][(long long)k0 * sxy + (long long)j0 * nx + i0] : 0.0;
+    TT q[4][9];  // z queue: q[v][m] = value at k - 4 + m (minus ref[v])
     const long long col = (long long)j * nx + i;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const long long off = (long long)wrap1(k0 - 4 + m, nz) * sxy + col;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) q[v][m] = src[v][off];
+        for (int v = 0; v < 4; ++v) q[v][m] = TT(src[v][off] - ref[v]);
     }
     const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
     const R mu_ref = R(P.mu), Ss = R(P.sutherland_s), Cp = R(P.Cp), Pr = R(P.Pr);
@@ -506,29 +516,28 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
         {
             const long long off = (long long)wrap1(k + 4, nz) * sxy + col;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) q[v][8] = src[v][off];
+            for (int v = 0; v < 4; ++v) q[v][8] = TT(src[v][off] - ref[v]);
         }
         for (int t = tid; t < VT_SX * VT_SY; t += VT_X * VT_Y) {
             const int ly = t / VT_SX, lx = t - ly * VT_SX;
             const long long off = plane + (long long)wrap1(j0 - VT_H + ly, ny) * nx + wrap1(i0 - VT_H + lx, nx);
 #pragma unroll
-            for (int v = 0; v < 4; ++v) tile[v][ly][lx] = src[v][off];
+            for (int v = 0; v < 4; ++v) tile[v][ly][lx] = TT(src[v][off] - ref[v]);
         }
         __syncthreads();
         const int cx = tx + VT_H, cy = ty + VT_H;
         R g[4][3];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const double c0 = kDeviation ? tile[v][cy][cx] : 0.0;
-            g[v][0] = dcentral<R, ORD>([&](int o) { return R(tile[v][cy][cx + o] - c0); }, dx);
-            g[v][1] = dcentral<R, ORD>([&](int o) { return R(tile[v][cy + o][cx] - c0); }, dy);
-            g[v][2] = dcentral<R, ORD>([&](int o) { return R(q[v][4 + o] - c0); }, dz);
+            g[v][0] = dcentral<R, ORD>([&](int o) { return tile[v][cy][cx + o]; }, dx);
+            g[v][1] = dcentral<R, ORD>([&](int o) { return tile[v][cy + o][cx]; }, dy);
+            g[v][2] = dcentral<R, ORD>([&](int o) { return q[v][4 + o]; }, dz);
         }
         const R du_dx = g[0][0], du_dy = g[0][1], du_dz = g[0][2];
         const R dv_dx = g[1][0], dv_dy = g[1][1], dv_dz = g[1][2];
         const R dw_dx = g[2][0], dw_dy = g[2][1], dw_dz = g[2][2];
         const R dT_dx = g[3][0], dT_dy = g[3][1], dT_dz = g[3][2];
-        const R mu = get_mu<R>(R(q[3][4]), mu_ref, Ss);
+        const R mu = get_mu<R>(R(ref[3]) + q[3][4], mu_ref, Ss);
         const R divU = du_dx + dv_dy + dw_dz;
         const R tau_xx = R(2.0) * mu * du_dx - R(2.0 / 3.0) * mu * divU;
         const R tau_yy = R(2.0) * mu * dv_dy - R(2.0 / 3.0) * mu * divU;
@@ -539,7 +548,7 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
         const R qx = mu * Cp / Pr * dT_dx;
         const R qy = mu * Cp / Pr * dT_dy;
         const R qz = mu * Cp / Pr * dT_dz;
-        const R u = R(q[0][4]), v = R(q[1][4]), w = R(q[2][4]);
+        const R u = R(ref[0]) + q[0][4], v = R(ref[1]) + q[1][4], w = R(ref[2]) + q[2][4];
         const long long id = plane + col;
         fv[0 * n + id] = tau_xx;
         fv[1 * n + id] = tau_yy;
