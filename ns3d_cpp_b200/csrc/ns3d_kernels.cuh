@@ -115,6 +115,8 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     // face-flux difference. The FP64 form keeps the reference's arithmetic.
     constexpr bool kDeviation = sizeof(R) < sizeof(double);
     double refp[5], refm[5];
+    const double inv_gm1 = kDeviation ? 1.0 / (P.gamma - 1.0) : 0.0;
+    const double inv_2g = kDeviation ? 1.0 / (2.0 * P.gamma) : 0.0;
     // Loads of one cell's primitives are issued a step before the cell is
     // split (`load_raw` into registers), so their latency hides behind the
     // reconstruction of the current face instead of stalling the march.
@@ -138,16 +140,8 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
             else
                 split_lf<R, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fp, Fm);
         } else {
-            double rr = raw[0];
-            const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
-            if (rr <= 0.0) rr = 1e-12;
-            double E, c, Fpd[5], Fmd[5];
-            p2c_Ec<double>(rr, u, v, w, p, P.gamma, E, c);
-            if constexpr (FVS == FV_SW)
-                split_sw<double, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, P.gamma,
-                                                               P.sw_eps, Fpd, Fmd);
-            else
-                split_lf<double, DIR == 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fpd, Fmd);
+            double Fpd[5], Fmd[5];
+            split_fast<FVS, DIR == 0, DIR == 1, DIR == 2>(P, inv_gm1, inv_2g, raw, Fpd, Fmd);
             if (set_ref) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
@@ -262,6 +256,8 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     (void)eps;
 
     double refp[5], refm[5];
+    const double inv_gm1 = kDeviation ? 1.0 / (P.gamma - 1.0) : 0.0;
+    const double inv_2g = kDeviation ? 1.0 / (2.0 * P.gamma) : 0.0;
     auto load_raw = [&](int chunk, double* raw) {
         const long long id = base + (chunk << 5) + lane;
         raw[0] = W.rho[id];
@@ -280,15 +276,8 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
             if constexpr (FVS == FV_SW) split_sw<R, 1, 0, 0>(rr, u, v, w, E, p, c, gamma, eps, Fp, Fm);
             else split_lf<R, 1, 0, 0>(rr, u, v, w, E, p, c, Fp, Fm);
         } else {
-            double rr = raw[0];
-            const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
-            if (rr <= 0.0) rr = 1e-12;
-            double E, c, Fpd[5], Fmd[5];
-            p2c_Ec<double>(rr, u, v, w, p, P.gamma, E, c);
-            if constexpr (FVS == FV_SW)
-                split_sw<double, 1, 0, 0>(rr, u, v, w, E, p, c, P.gamma, P.sw_eps, Fpd, Fmd);
-            else
-                split_lf<double, 1, 0, 0>(rr, u, v, w, E, p, c, Fpd, Fmd);
+            double Fpd[5], Fmd[5];
+            split_fast<FVS, 1, 0, 0>(P, inv_gm1, inv_2g, raw, Fpd, Fmd);
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 Fp[q] = R(Fpd[q] - refp[q]);
@@ -300,14 +289,8 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     if constexpr (kDeviation) {
         double raw[5];
         load_raw(0, raw);
-        double rr = raw[0];
-        if (rr <= 0.0) rr = 1e-12;
-        double E, c, Fpd[5], Fmd[5];
-        p2c_Ec<double>(rr, raw[1], raw[2], raw[3], raw[4], P.gamma, E, c);
-        if constexpr (FVS == FV_SW)
-            split_sw<double, 1, 0, 0>(rr, raw[1], raw[2], raw[3], E, raw[4], c, P.gamma, P.sw_eps, Fpd, Fmd);
-        else
-            split_lf<double, 1, 0, 0>(rr, raw[1], raw[2], raw[3], E, raw[4], c, Fpd, Fmd);
+        double Fpd[5], Fmd[5];
+        split_fast<FVS, 1, 0, 0>(P, inv_gm1, inv_2g, raw, Fpd, Fmd);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             refp[q] = __shfl_sync(0xffffffffu, Fpd[q], 0);
