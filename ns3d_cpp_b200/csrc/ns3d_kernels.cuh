@@ -660,6 +660,96 @@ __device__ __forceinline__ void block_min_to(double v, unsigned long long* dst) 
 // Wn: output. Stage 3 may write Wn == W0 in place (each thread reads its own
 // cell of W0 before writing it), so no pointer here is __restrict__.
 // ---------------------------------------------------------------------------
+// The FP32-stencil form (R = float) keeps the state in double but takes the
+// divisions by rho as multiplications by one Newton-refined reciprocal (see
+// rcp_nr): its rhs already carries float rounding, so the reference's exact
+// cons->prim->cons round trip is only kept in the FP64 form.
+__device__ __forceinline__ void prim2cons_fast(const StateView& W, long long id, double inv_gm1,
+                                               double U[5]) {
+    double rr = W.rho[id];
+    if (rr <= 0.0) rr = 1e-12;
+    const double u = W.u[id], v = W.v[id], w = W.w[id], p = W.p[id];
+    U[0] = rr;
+    U[1] = rr * u;
+    U[2] = rr * v;
+    U[3] = rr * w;
+    U[4] = p * inv_gm1 + rr * (0.5 * (u * u + v * v + w * w));
+}
+
+// Shu-Osher stage of one cell from its rhs r, conservedToPrimitive of the
+// result and, after stage 3, the positivity test and the CFL candidate
+// (folded into `cand` with std::min semantics: a NaN never wins).
+template <class R, int STAGE>
+__device__ __forceinline__ void stage_cell(const DevParams& P, const StateView& Wc,
+                                           const StateView& W0, long long id, const R r[5],
+                                           double dt, const StateOut& Wn, Ctrl* ctrl,
+                                           double& cand) {
+    constexpr bool kFast = sizeof(R) < sizeof(double);
+    const double gamma = P.gamma;
+    double U0[5], U[5];
+    if constexpr (kFast) {
+        const double inv_gm1 = 1.0 / (gamma - 1.0);
+        prim2cons_fast(W0, id, inv_gm1, U0);
+        if (STAGE != 1) prim2cons_fast(Wc, id, inv_gm1, U);
+    } else {
+        prim2cons_cell(W0, id, gamma, U0);
+        if (STAGE != 1) prim2cons_cell(Wc, id, gamma, U);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const double rq = double(r[q]);
+        if (STAGE == 1)
+            U[q] = U0[q] + dt * rq;
+        else if (STAGE == 2)
+            U[q] = 0.75 * U0[q] + 0.25 * (U[q] + dt * rq);
+        else
+            U[q] = (1.0 / 3.0) * U0[q] + (2.0 / 3.0) * (U[q] + dt * rq);
+    }
+    // conservedToPrimitive (field_structures.h:405-427)
+    double rr = U[0];
+    if (rr <= 0.0) rr = 1e-12;
+    double u, v, w, p, T;
+    if constexpr (kFast) {
+        const double ir = rcp_nr(rr);
+        u = U[1] * ir;
+        v = U[2] * ir;
+        w = U[3] * ir;
+        p = (gamma - 1.0) * (U[4] - rr * (0.5 * (u * u + v * v + w * w)));
+        T = p * ir * (1.0 / P.Rgas);
+    } else {
+        u = U[1] / rr;
+        v = U[2] / rr;
+        w = U[3] / rr;
+        const double kinetic = 0.5 * (u * u + v * v + w * w);
+        const double e_internal = U[4] / rr - kinetic;
+        p = (gamma - 1.0) * rr * e_internal;
+        T = p / (rr * P.Rgas);  // primitiveToConserved's T
+    }
+    Wn.rho[id] = rr;
+    Wn.u[id] = u;
+    Wn.v[id] = v;
+    Wn.w[id] = w;
+    Wn.p[id] = p;
+    Wn.T[id] = T;
+    if (STAGE == 3) {
+        // range_kutta.cpp:154 tests rho <= 0 || p <= 0 || T <= 0, which a
+        // NaN passes; the negated form below also reports NaN.
+        if (!(rr > 0.0) || !(p > 0.0) || !(T > 0.0)) atomicMin(&ctrl->bad_cell, id);
+        double c;
+        if constexpr (kFast) {
+            const double a = sqrt_nr(gamma * p * rcp_nr(rr));
+            const double cx = P.dx * rcp_nr(fabs(u) + a);
+            const double cy = P.dy * rcp_nr(fabs(v) + a);
+            const double cz = P.dz * rcp_nr(fabs(w) + a);
+            c = (cz < cy) ? cz : cy;
+            c = (c < cx) ? c : cx;
+        } else {
+            c = cfl_candidate(P, rr, u, v, w, p);
+        }
+        cand = (c < cand) ? c : cand;
+    }
+}
+
 template <class R, int ORD, int STAGE>
 __global__ void __launch_bounds__(128)
 k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
@@ -673,41 +763,7 @@ k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
     if (live) {
         R r[5];
         cell_rhs<R, ORD>(P, tacc, fv, i, j, k, id, r);
-        const double dt = ctrl->dt;
-        const double gamma = P.gamma;
-        double U0[5], U[5];
-        prim2cons_cell(W0, id, gamma, U0);
-        if (STAGE != 1) prim2cons_cell(Wc, id, gamma, U);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            const double rq = double(r[q]);
-            if (STAGE == 1)
-                U[q] = U0[q] + dt * rq;
-            else if (STAGE == 2)
-                U[q] = 0.75 * U0[q] + 0.25 * (U[q] + dt * rq);
-            else
-                U[q] = (1.0 / 3.0) * U0[q] + (2.0 / 3.0) * (U[q] + dt * rq);
-        }
-        // conservedToPrimitive (field_structures.h:405-427)
-        double rr = U[0];
-        if (rr <= 0.0) rr = 1e-12;
-        const double u = U[1] / rr, v = U[2] / rr, w = U[3] / rr;
-        const double kinetic = 0.5 * (u * u + v * v + w * w);
-        const double e_internal = U[4] / rr - kinetic;
-        const double p = (gamma - 1.0) * rr * e_internal;
-        const double T = p / (rr * P.Rgas);  // primitiveToConserved's T
-        Wn.rho[id] = rr;
-        Wn.u[id] = u;
-        Wn.v[id] = v;
-        Wn.w[id] = w;
-        Wn.p[id] = p;
-        Wn.T[id] = T;
-        if (STAGE == 3) {
-            // range_kutta.cpp:154 tests rho <= 0 || p <= 0 || T <= 0, which a
-            // NaN passes; the negated form below also reports NaN.
-            if (!(rr > 0.0) || !(p > 0.0) || !(T > 0.0)) atomicMin(&ctrl->bad_cell, id);
-            cand = cfl_candidate(P, rr, u, v, w, p);
-        }
+        stage_cell<R, STAGE>(P, Wc, W0, id, r, ctrl->dt, Wn, ctrl, cand);
     }
     if (STAGE == 3) block_min_to(cand, &ctrl->dtmin_bits);
 }
@@ -745,7 +801,6 @@ k_update_25d(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc
     }
     const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
     const double dt = ctrl->dt;
-    const double gamma = P.gamma;
     double cand = CFL_INIT;
     for (int k = k0; k < k1; ++k) {
         const long long plane = (long long)k * sxy;
@@ -780,37 +835,7 @@ k_update_25d(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc
         }
 #pragma unroll
         for (int qq = 0; qq < 5; ++qq) r[qq] += -tacc[qq * n + id];
-        double U0[5], U[5];
-        prim2cons_cell(W0, id, gamma, U0);
-        if (STAGE != 1) prim2cons_cell(Wc, id, gamma, U);
-#pragma unroll
-        for (int qq = 0; qq < 5; ++qq) {
-            const double rq = double(r[qq]);
-            if (STAGE == 1)
-                U[qq] = U0[qq] + dt * rq;
-            else if (STAGE == 2)
-                U[qq] = 0.75 * U0[qq] + 0.25 * (U[qq] + dt * rq);
-            else
-                U[qq] = (1.0 / 3.0) * U0[qq] + (2.0 / 3.0) * (U[qq] + dt * rq);
-        }
-        double rr = U[0];
-        if (rr <= 0.0) rr = 1e-12;
-        const double u = U[1] / rr, v = U[2] / rr, w = U[3] / rr;
-        const double kinetic = 0.5 * (u * u + v * v + w * w);
-        const double e_internal = U[4] / rr - kinetic;
-        const double p = (gamma - 1.0) * rr * e_internal;
-        const double T = p / (rr * P.Rgas);
-        Wn.rho[id] = rr;
-        Wn.u[id] = u;
-        Wn.v[id] = v;
-        Wn.w[id] = w;
-        Wn.p[id] = p;
-        Wn.T[id] = T;
-        if (STAGE == 3) {
-            if (!(rr > 0.0) || !(p > 0.0) || !(T > 0.0)) atomicMin(&ctrl->bad_cell, id);
-            const double c = cfl_candidate(P, rr, u, v, w, p);
-            cand = (c < cand) ? c : cand;
-        }
+        stage_cell<R, STAGE>(P, Wc, W0, id, r, dt, Wn, ctrl, cand);
 #pragma unroll
         for (int v2 = 0; v2 < 4; ++v2)
 #pragma unroll
