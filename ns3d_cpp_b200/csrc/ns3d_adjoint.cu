@@ -45,17 +45,22 @@ __device__ __forceinline__ void load_w5(const StateView& W, long long id, double
     w[4] = W.p[id];
 }
 
+// Forward split at the windows' cells, with Newton-refined reciprocal and
+// square roots (split_fast, two steps: about an ulp).
 template <int FVS, int DIR>
 __device__ __forceinline__ void split_fwd(const double* w5, const DevParams& P, double* Fp,
                                           double* Fm) {
-    double E, c;
-    p2c_Ec<double>(w5[0], w5[1], w5[2], w5[3], w5[4], P.gamma, E, c);
-    if constexpr (FVS == FV_SW)
-        split_sw<double, DIR == 0, DIR == 1, DIR == 2>(w5[0], w5[1], w5[2], w5[3], E, w5[4], c,
-                                                       P.gamma, P.sw_eps, Fp, Fm);
-    else
-        split_lf<double, DIR == 0, DIR == 1, DIR == 2>(w5[0], w5[1], w5[2], w5[3], E, w5[4], c,
-                                                       Fp, Fm);
+    split_fast<FVS, DIR == 0, DIR == 1, DIR == 2, 2>(P, 1.0 / (P.gamma - 1.0), 0.5 / P.gamma,
+                                                     w5, Fp, Fm);
+}
+
+// Index of face/cell position f of a line in the split-flux cotangent array G.
+// x lines (threads over j) use a j-fastest layout so that a warp's stores are
+// contiguous; y and z lines (threads over i) use the cell index itself.
+template <int DIR>
+__device__ __forceinline__ long long g_index(const DevParams& P, int i, int j, int k) {
+    if constexpr (DIR == 0) return ((long long)k * P.nx + i) * P.ny + j;
+    else return ((long long)k * P.ny + j) * P.nx + i;
 }
 
 // Reconstruction VJP of every face: marches a line segment like k_sweep,
@@ -103,7 +108,8 @@ k_adj_face(DevParams P, StateView W, const double* __restrict__ lamR, double* __
         double w5[5];
         load_w5(W, idx(f - MID + S - 1), w5);
         split_fwd<FVS, DIR>(w5, P, fp[S - 1], fm[S - 1]);
-        const long long fid = idx(f), nid = idx(f + 1);
+        const long long nid = idx(f + 1);
+        const long long fid = DIR == 0 ? g_index<0>(P, f, t0, blockIdx.y) : idx(f);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             const double lr_next = lamR[q * n + nid];
@@ -142,12 +148,20 @@ __global__ void __launch_bounds__(128)
 k_adj_cell(DevParams P, StateView W, const double* __restrict__ G, double* __restrict__ lamW) {
     constexpr int S = Stencil<RC>::S;
     constexpr int MID = (S - 1) / 2;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.nx) return;
-    const int j = blockIdx.y, k = blockIdx.z;
+    // x: threads over j (G's x layout is j-fastest); y, z: threads over i
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (DIR == 0 ? P.ny : P.nx)) return;
+    const int i = DIR == 0 ? (int)blockIdx.y : t, j = DIR == 0 ? t : (int)blockIdx.y;
+    const int k = blockIdx.z;
     const long long n = P.n;
     const long long id = ((long long)k * P.ny + j) * P.nx + i;
-    const Line L = line_of<DIR>(P, i, j, k, id);
+    const int pos = DIR == 0 ? i : (DIR == 1 ? j : k);
+    const int len = DIR == 0 ? P.nx : (DIR == 1 ? P.ny : P.nz);
+    auto gat = [&](int s) {
+        const int w = wrap1(s, len);
+        return DIR == 0 ? g_index<0>(P, w, j, k) : (DIR == 1 ? g_index<1>(P, i, w, k)
+                                                             : g_index<2>(P, i, j, w));
+    };
     double gp[5], gm[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
@@ -155,9 +169,9 @@ k_adj_cell(DevParams P, StateView W, const double* __restrict__ G, double* __res
 #pragma unroll
         for (int m = 0; m < S; ++m) {
             // cell c = f - MID + m in the plus window of face f = c + MID - m
-            sp += G[((long long)(0 * S + m) * 5 + q) * n + L.at(L.pos + MID - m)];
+            sp += G[((long long)(0 * S + m) * 5 + q) * n + gat(pos + MID - m)];
             // cell c = f - MID + (S-1-m) in the minus window of face f = c + MID - S + 1 + m
-            sm += G[((long long)(1 * S + m) * 5 + q) * n + L.at(L.pos + MID - S + 1 + m)];
+            sm += G[((long long)(1 * S + m) * 5 + q) * n + gat(pos + MID - S + 1 + m)];
         }
         gp[q] = sp;
         gm[q] = sm;
@@ -347,8 +361,10 @@ cudaError_t adj_dir(const LaunchCfg& L, StateView W, const double* lamR, double*
     k_adj_face<DIR, FVS, RC><<<grid, th, 0, L.stream>>>(P, W, lamR, G, seg);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const int tc = detail::threads_for(P.nx);
-    k_adj_cell<DIR, FVS, RC><<<detail::cell_grid(P, tc), tc, 0, L.stream>>>(P, W, G, lamW);
+    const int cext = DIR == 0 ? P.ny : P.nx;
+    const int tc = detail::threads_for(cext);
+    const dim3 cg((cext + tc - 1) / tc, DIR == 0 ? P.nx : P.ny, P.nz);
+    k_adj_cell<DIR, FVS, RC><<<cg, tc, 0, L.stream>>>(P, W, G, lamW);
     return cudaGetLastError();
 }
 

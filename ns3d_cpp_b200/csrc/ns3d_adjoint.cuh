@@ -11,6 +11,7 @@ namespace ns3d {
 // d rec / d a_j of weno5(a0..a4), times lam, added to g[0..4].
 // rec = sum w_k p_k, w_k = alpha_k / sum alpha, alpha_k = d_k / (eps + beta_k)^2:
 // d rec / d beta_l = -2 w_l (p_l - rec) / (eps + beta_l).
+// Reciprocals are Newton-refined estimates (rcp_nr, two steps: about an ulp).
 __device__ __forceinline__ void weno5_vjp(const double* a, double lam, double* g) {
     const double eps = 1e-6;
     const double a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4];
@@ -20,13 +21,13 @@ __device__ __forceinline__ void weno5_vjp(const double* a, double lam, double* g
     const double b0 = 13.0 / 12.0 * D0 * D0 + 0.25 * E0 * E0;
     const double b1 = 13.0 / 12.0 * D1 * D1 + 0.25 * E1 * E1;
     const double b2 = 13.0 / 12.0 * D2 * D2 + 0.25 * E2 * E2;
-    const double r0 = 1.0 / (eps + b0), r1 = 1.0 / (eps + b1), r2 = 1.0 / (eps + b2);
+    const double r0 = rcp_nr<2>(eps + b0), r1 = rcp_nr<2>(eps + b1), r2 = rcp_nr<2>(eps + b2);
     const double al0 = 0.1 * r0 * r0, al1 = 0.6 * r1 * r1, al2 = 0.3 * r2 * r2;
-    const double inv = 1.0 / (al0 + al1 + al2);
+    const double inv = rcp_nr<2>(al0 + al1 + al2);
     const double w0 = al0 * inv, w1 = al1 * inv, w2 = al2 * inv;
-    const double p0 = (2.0 * a0 - 7.0 * a1 + 11.0 * a2) / 6.0;
-    const double p1 = (-a1 + 5.0 * a2 + 2.0 * a3) / 6.0;
-    const double p2 = (2.0 * a2 + 5.0 * a3 - a4) / 6.0;
+    const double p0 = (2.0 * a0 - 7.0 * a1 + 11.0 * a2) * (1.0 / 6.0);
+    const double p1 = (-a1 + 5.0 * a2 + 2.0 * a3) * (1.0 / 6.0);
+    const double p2 = (2.0 * a2 + 5.0 * a3 - a4) * (1.0 / 6.0);
     const double rec = w0 * p0 + w1 * p1 + w2 * p2;
     const double s0 = -2.0 * w0 * (p0 - rec) * r0 * lam;
     const double s1 = -2.0 * w1 * (p1 - rec) * r1 * lam;
@@ -59,15 +60,17 @@ __device__ __forceinline__ void reconstruct_vjp(const double* s, const double* l
 
 // Split fluxes of one primitive state w = (rho,u,v,w,p) along DIR and the
 // VJP: gw[5] += (dF+/dw)^T gp + (dF-/dw)^T gm. The forward part repeats
-// p2c_Ec + split_sw / split_lf in FP64.
+// p2c_Ec + split_sw / split_lf in FP64, with Newton-refined reciprocals and
+// square roots (rcp_nr, sqrt_nr, two steps) in place of IEEE division and sqrt.
 template <int FVS, int DIR>
 __device__ __forceinline__ void split_vjp(const double* w5, double gamma, double eps,
                                           const double* gp, const double* gm, double* gw) {
     const double rho = w5[0], u = w5[1], v = w5[2], w = w5[3], p = w5[4];
     const double vel[3] = {u, v, w};
     const double k = 0.5 * (u * u + v * v + w * w);
+    const double ir = rcp_nr<2>(rho);
     const double E = p / (gamma - 1.0) + rho * k;
-    const double c = sqrt(gamma * p / rho);
+    const double c = sqrt_nr<2>(gamma * p * ir);
     const double un = vel[DIR];
     double grho = 0.0, gvel[3] = {0.0, 0.0, 0.0}, gp_ = 0.0, gE = 0.0, gc = 0.0, gk = 0.0,
            gun = 0.0;
@@ -76,13 +79,13 @@ __device__ __forceinline__ void split_vjp(const double* w5, double gamma, double
         double a[3], lp[3], lm[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            a[i] = eps > 0.0 ? sqrt(l[i] * l[i] + eps * eps) : fabs(l[i]);
+            a[i] = eps > 0.0 ? sqrt_nr<2>(l[i] * l[i] + eps * eps) : fabs(l[i]);
             lp[i] = 0.5 * (l[i] + a[i]);
             lm[i] = 0.5 * (l[i] - a[i]);
         }
         const double S1p = lp[0] + lp[2], S1m = lm[0] + lm[2];
         const double S2p = lp[2] - lp[0], S2m = lm[2] - lm[0];
-        const double H = (E + p) / rho;
+        const double H = (E + p) * ir;
         const double ga1 = rho / (2.0 * gamma), ga2 = 2.0 * (gamma - 1.0);
         const double V = k;
         double gS1p = 0, gS1m = 0, gS2p = 0, gS2m = 0, glp2 = 0, glm2 = 0, gH = 0, gV = 0,
@@ -129,14 +132,14 @@ __device__ __forceinline__ void split_vjp(const double* w5, double gamma, double
         for (int i = 0; i < 3; ++i) {
             const double ga = 0.5 * (glp[i] - glm[i]);
             gl[i] = 0.5 * (glp[i] + glm[i]);
-            const double dadl = eps > 0.0 ? l[i] / a[i] : (l[i] > 0.0 ? 1.0 : (l[i] < 0.0 ? -1.0 : 0.0));
+            const double dadl = eps > 0.0 ? l[i] * rcp_nr<2>(a[i]) : (l[i] > 0.0 ? 1.0 : (l[i] < 0.0 ? -1.0 : 0.0));
             gl[i] += ga * dadl;
         }
         gun += gl[0] + gl[1] + gl[2];
         gc += -gl[0] + gl[2];
-        gE += gH / rho;
-        gp_ += gH / rho;
-        grho += -gH * H / rho;
+        gE += gH * ir;
+        gp_ += gH * ir;
+        grho += -gH * H * ir;
         gk += gV;
         grho += gga1 / (2.0 * gamma);
     } else {
@@ -181,8 +184,8 @@ __device__ __forceinline__ void split_vjp(const double* w5, double gamma, double
     }
     gvel[DIR] += gun;
     // c = sqrt(gamma p / rho)
-    gp_ += gc * gamma / (2.0 * c * rho);
-    grho += -gc * c / (2.0 * rho);
+    gp_ += gc * gamma * 0.5 * rcp_nr<2>(c) * ir;
+    grho += -gc * c * 0.5 * ir;
     // E = p/(gamma-1) + rho k
     gp_ += gE / (gamma - 1.0);
     grho += gE * k;

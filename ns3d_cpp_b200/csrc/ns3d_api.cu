@@ -481,12 +481,15 @@ ns3d_status compute_sums(ns3d_ctx* ctx, double out[NSUMS]) {
 namespace ns3d {
 
 // Measured at 256^3 (B200): the 2.5-D viscous flux with 16 planes per block is
-// the fastest shape (FP64 1.15 -> 1.01 ms, FP32 unchanged).
+// the fastest shape (FP64 1.15 -> 1.01 ms, FP32 unchanged); smaller boxes take
+// fewer planes per block (detail::zb_for) so that the grid fills the SMs.
 void default_tiling(LaunchCfg& L) {
-    L.zb = 16;
+    L.zb = 0;
     L.tiled = 1;
     if (const char* e = std::getenv("NS3D_TILE_ZB")) L.zb = std::atoi(e);
     if (const char* e = std::getenv("NS3D_TILED")) L.tiled = std::atoi(e);
+    if (const char* e = std::getenv("NS3D_SEG"))
+        for (int d = 0; d < 3; ++d) L.seg[d] = std::atoi(e);
 }
 
 ns3d_status build_launch_cfg(const ns3d_params* p, LaunchCfg* L, std::string* msg) {

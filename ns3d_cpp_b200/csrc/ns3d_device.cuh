@@ -133,29 +133,38 @@ __device__ __forceinline__ void split_lf(R rho, R u, R v, R w, R E, R p, R c, R 
 // taken from the hardware estimates refined by one Newton-Raphson step:
 //   1/b:     x <- x + x (1 - b x)
 //   sqrt(b): s = b y (y ~ 1/sqrt b), s <- s + (y/2) (b - s^2)   (Heron)
-// Each step squares the estimate's relative error (2^-23 or better on entry),
-// leaving ~1e-14, far below the float rounding of the deviations that the
-// reconstructions see (measured: the same FP32-vs-FP64 error after 100 steps
-// at 256^3 as with IEEE operations). The FP64 form keeps the reference's
-// IEEE divisions and square roots.
+// Each step squares the estimate's relative error (2^-23 or better on entry):
+// one step leaves ~1e-14, far below the float rounding of the deviations that
+// the FP32 form's reconstructions see (measured: the same FP32-vs-FP64 error
+// after 100 steps at 256^3 as with IEEE operations); two steps (with the
+// 1/sqrt estimate refined first, y <- y (3 - b y^2) / 2) leave about an ulp,
+// which the FP64 adjoint needs because the entropy fix's 0.5 (l - sqrt(l^2 +
+// eps^2)) amplifies the square root's error by ~l^2/eps^2. The FP64 forward
+// form keeps the reference's IEEE divisions and square roots.
 // ---------------------------------------------------------------------------
+template <int STEPS = 1>
 __device__ __forceinline__ double rcp_nr(double b) {
     double x;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(b));
-    return fma(x, fma(-b, x, 1.0), x);
+#pragma unroll
+    for (int s = 0; s < STEPS; ++s) x = fma(x, fma(-b, x, 1.0), x);
+    return x;
 }
 
+template <int STEPS = 1>
 __device__ __forceinline__ double sqrt_nr(double b) {
     // zero, negative, NaN and huge arguments take the IEEE path
     if (!(b > 0.0 && b < 1.0e300)) return sqrt(b);
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+#pragma unroll
+    for (int s = 1; s < STEPS; ++s) y = y * fma(-0.5 * b * y, y, 1.5);
     const double s = b * y;
     return fma(0.5 * y, fma(-s, s, b), s);
 }
 
 // raw = (rho, u, v, w, p) of one cell; inv_gm1 = 1/(gamma-1), inv_2g = 1/(2 gamma).
-template <int FVS, int N1, int N2, int N3>
+template <int FVS, int N1, int N2, int N3, int STEPS = 1>
 __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, double inv_2g,
                                            const double* raw, double Fp[5], double Fm[5]) {
     const double n1 = N1, n2 = N2, n3 = N3;
@@ -163,17 +172,17 @@ __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, d
     if (rho <= 0.0) rho = 1e-12;
     const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
     const double gamma = P.gamma;
-    const double ir = rcp_nr(rho);
+    const double ir = rcp_nr<STEPS>(rho);
     const double kinetic = 0.5 * (u * u + v * v + w * w);
     const double E = rho * (p * ir * inv_gm1 + kinetic);
-    const double c = sqrt_nr(gamma * p * ir);
+    const double c = sqrt_nr<STEPS>(gamma * p * ir);
     const double un = u * n1 + v * n2 + w * n3;
     if constexpr (FVS == FV_SW) {
         const double eps = P.sw_eps;
         const double l1 = un - c, l2 = un, l3 = un + c;
-        const double a1 = eps > 0.0 ? sqrt_nr(l1 * l1 + eps * eps) : fabs(l1);
-        const double a2 = eps > 0.0 ? sqrt_nr(l2 * l2 + eps * eps) : fabs(l2);
-        const double a3 = eps > 0.0 ? sqrt_nr(l3 * l3 + eps * eps) : fabs(l3);
+        const double a1 = eps > 0.0 ? sqrt_nr<STEPS>(l1 * l1 + eps * eps) : fabs(l1);
+        const double a2 = eps > 0.0 ? sqrt_nr<STEPS>(l2 * l2 + eps * eps) : fabs(l2);
+        const double a3 = eps > 0.0 ? sqrt_nr<STEPS>(l3 * l3 + eps * eps) : fabs(l3);
         const double l1p = 0.5 * (l1 + a1), l1m = 0.5 * (l1 - a1);
         const double l2p = 0.5 * (l2 + a2), l2m = 0.5 * (l2 - a2);
         const double l3p = 0.5 * (l3 + a3), l3m = 0.5 * (l3 - a3);

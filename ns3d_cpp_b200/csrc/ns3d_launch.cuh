@@ -15,11 +15,11 @@ struct LaunchCfg {
     int rc;       // RC_* of the reconstruction
     int seg[3];   // cells per thread segment along x, y, z
     cudaStream_t stream;
-    int zb;       // planes per block of the 2.5-D viscous kernels
+    int zb;       // planes per block of the 2.5-D viscous kernels (0: from the grid)
     int tiled;    // bit 0: 2.5-D visc_flux, bit 1: 2.5-D update (when the box tiles)
 };
 
-// Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED for tuning.
+// Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED / NS3D_SEG for tuning.
 void default_tiling(LaunchCfg& L);
 
 // One inviscid sweep (dir 0, 1, 2 in this order per RHS evaluation).
@@ -40,15 +40,13 @@ inline int threads_for(int ext) { return ext >= 128 ? 128 : (ext >= 64 ? 64 : 32
 inline dim3 cell_grid(const DevParams& P, int th) { return dim3((P.nx + th - 1) / th, P.ny, P.nz); }
 
 // Cells per marching segment: long segments amortise the S-1 halo splits at
-// the segment start, short ones give enough threads to fill 148 SMs. Aim for
-// about two waves of 16 warps per SM, within [16, 64] cells (and <= len).
+// the segment start, short ones give enough threads to fill 148 SMs. One cell
+// per 1024 lines, within [1, 64] (and <= len): the fastest lengths measured on
+// a B200 were 1 at 32^3 (1024 lines), 4 at 64^3, 16 at 128^3 and 64 at 256^3.
 inline int segment_for(int len, long long lines) {
-    const long long target = 148LL * 512 * 2;
-    long long nseg = (target + lines - 1) / lines;
-    int seg = (int)((len + nseg - 1) / nseg);
-    seg = (seg + 7) / 8 * 8;
-    seg = seg < 16 ? 16 : (seg > 64 ? 64 : seg);
-    return seg > len ? len : seg;
+    long long seg = lines / 1024;
+    seg = seg < 1 ? 1 : (seg > 64 ? 64 : seg);
+    return seg > len ? len : (int)seg;
 }
 
 }  // namespace detail
@@ -105,10 +103,20 @@ cudaError_t launch_sweep(const LaunchCfg& L, int dir, StateView W, R* tacc, cons
 
 namespace detail {
 inline bool tiles_25d(const LaunchCfg& L, int bit) {
-    return (L.tiled & bit) && L.zb > 0 && L.P.nx % VT_X == 0 && L.P.ny % VT_Y == 0;
+    return (L.tiled & bit) && L.zb >= 0 && L.P.nx % VT_X == 0 && L.P.ny % VT_Y == 0;
+}
+// Planes per block of the 2.5-D kernels: L.zb when set, else 16 halved until
+// the grid has at least 4 blocks per SM (32^3: 1 plane, 128^3: 8, 256^3: 16).
+inline int zb_for(const LaunchCfg& L) {
+    if (L.zb > 0) return L.zb;
+    const long long tiles = (long long)(L.P.nx / VT_X) * (L.P.ny / VT_Y);
+    int zb = 16;
+    while (zb > 1 && tiles * ((L.P.nz + zb - 1) / zb) < 4 * 148) zb >>= 1;
+    return zb;
 }
 inline dim3 grid_25d(const LaunchCfg& L) {
-    return dim3(L.P.nx / VT_X, L.P.ny / VT_Y, (L.P.nz + L.zb - 1) / L.zb);
+    const int zb = zb_for(L);
+    return dim3(L.P.nx / VT_X, L.P.ny / VT_Y, (L.P.nz + zb - 1) / zb);
 }
 }  // namespace detail
 
@@ -117,9 +125,9 @@ cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl*
     if (detail::tiles_25d(L, 1)) {
         const dim3 g = detail::grid_25d(L), b(VT_X, VT_Y);
         switch (L.P.vis_order) {
-        case 4: k_visc_flux_25d<R, 4><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, L.zb); break;
-        case 6: k_visc_flux_25d<R, 6><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, L.zb); break;
-        default: k_visc_flux_25d<R, 8><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, L.zb); break;
+        case 4: k_visc_flux_25d<R, 4><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for(L)); break;
+        case 6: k_visc_flux_25d<R, 6><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for(L)); break;
+        default: k_visc_flux_25d<R, 8><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for(L)); break;
         }
         return cudaGetLastError();
     }
@@ -138,9 +146,9 @@ static cudaError_t update_ord(const LaunchCfg& L, int stage, StateView Wc, State
                               const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl) {
     if (detail::tiles_25d(L, 2)) {
         const dim3 g = detail::grid_25d(L), b(VT_X, VT_Y);
-        if (stage == 1) k_update_25d<R, ORD, 1><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, L.zb);
-        else if (stage == 2) k_update_25d<R, ORD, 2><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, L.zb);
-        else k_update_25d<R, ORD, 3><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, L.zb);
+        if (stage == 1) k_update_25d<R, ORD, 1><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, detail::zb_for(L));
+        else if (stage == 2) k_update_25d<R, ORD, 2><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, detail::zb_for(L));
+        else k_update_25d<R, ORD, 3><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, detail::zb_for(L));
         return cudaGetLastError();
     }
     const int th = detail::threads_for(L.P.nx);
