@@ -186,7 +186,10 @@ def kernel_bytes_per_cell(cls: str, rsize: int) -> float:
     if cls == "visc_flux":
         return 4 * 8 + 9 * rsize
     if cls == "update":
-        return 2 * w + 5 * rsize + 9 * rsize + 6 * 8
+        # current + recorded state (stage 1 reads only the recorded one: the
+        # mean over the three stages is 5/3 state reads), T_acc, the 9 viscous
+        # flux blocks, 6 doubles written
+        return (5.0 / 3.0) * w + 5 * rsize + 9 * rsize + 6 * 8
     return 0.0
 
 
@@ -381,12 +384,16 @@ def our_arm(args, rank, world, local):
     tr = ncu_traffic()
     traffic = tr.get(f"fp32acc64/{dom}")
     traffic = None if traffic is None else traffic * 1e9 * (ncell / 256 ** 3)
+    # algorithmic bytes of the captured launch (the update capture is a stage-2 launch)
+    cap_alg = tr.get(f"fp32acc64/{dom}/alg_bytes_per_cell")
+    traffic_alg = None if traffic is None else (cap_alg or kernel_bytes_per_cell(dom, rsize)) * ncell
     ach = kern[dom]["achieved_gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
                 "alg_bytes_per_cell": kernel_bytes_per_cell(dom, rsize),
                 "alg_bytes_per_launch": kern[dom]["alg_bytes_per_launch"],
-                "traffic_source": tr.get("source") if traffic is not None else None}
+                "traffic_source": tr.get("source") if traffic is not None else None,
+                "traffic_alg_bytes": traffic_alg}
     step_ach = STEP_BYTES_PER_CELL * ncell * (value / world) / 1e9
     roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s",
                      "frac": step_ach / peak, "alg_bytes_per_cell_step": STEP_BYTES_PER_CELL}
