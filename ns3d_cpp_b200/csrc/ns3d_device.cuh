@@ -259,6 +259,77 @@ __device__ __forceinline__ float weno5(float f0, float f1, float f2, float f3, f
     return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
+// Approximate float reciprocal (the hardware estimate, ~1 ulp).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Two float weno5 reconstructions at once in sm_100's paired FP32 arithmetic
+// (one FFMA2/FADD2/FMUL2 instruction per operation on both lanes of a float2):
+// the same indicators, weights, candidate stencils and normalised sum as
+// weno5(float), operation for operation; only the approximate reciprocals run
+// per lane. The sweeps are instruction-issue bound, so halving the
+// reconstructions' instruction count shortens them.
+__device__ __forceinline__ float2 weno5x2(float2 f0, float2 f1, float2 f2, float2 f3, float2 f4) {
+    auto c = [](float v) { return make_float2(v, v); };
+    const float2 t0 = __fadd2_rn(__ffma2_rn(c(-2.f), f1, f0), f2);
+    const float2 s0 = __ffma2_rn(c(3.f), f2, __ffma2_rn(c(-4.f), f1, f0));
+    const float2 t1 = __fadd2_rn(__ffma2_rn(c(-2.f), f2, f1), f3);
+    const float2 s1 = __ffma2_rn(c(-1.f), f3, f1);
+    const float2 t2 = __fadd2_rn(__ffma2_rn(c(-2.f), f3, f2), f4);
+    const float2 s2 = __fadd2_rn(__ffma2_rn(c(-4.f), f3, __fmul2_rn(c(3.f), f2)), f4);
+    // z = eps + (13/12 t^2 + s^2 / 4)
+    const float2 z0 = __fadd2_rn(c(1e-6f), __ffma2_rn(__fmul2_rn(c(13.f / 12.f), t0), t0,
+                                                      __fmul2_rn(__fmul2_rn(c(0.25f), s0), s0)));
+    const float2 z1 = __fadd2_rn(c(1e-6f), __ffma2_rn(__fmul2_rn(c(13.f / 12.f), t1), t1,
+                                                      __fmul2_rn(__fmul2_rn(c(0.25f), s1), s1)));
+    const float2 z2 = __fadd2_rn(c(1e-6f), __ffma2_rn(__fmul2_rn(c(13.f / 12.f), t2), t2,
+                                                      __fmul2_rn(__fmul2_rn(c(0.25f), s2), s2)));
+    const float2 y0 = __fmul2_rn(z0, z0), y1 = __fmul2_rn(z1, z1), y2 = __fmul2_rn(z2, z2);
+    const float2 a0 = __fmul2_rn(c(0.1f), make_float2(rcp_approx(y0.x), rcp_approx(y0.y)));
+    const float2 a1 = __fmul2_rn(c(0.6f), make_float2(rcp_approx(y1.x), rcp_approx(y1.y)));
+    const float2 a2 = __fmul2_rn(c(0.3f), make_float2(rcp_approx(y2.x), rcp_approx(y2.y)));
+    const float2 sum = __fadd2_rn(__fadd2_rn(a0, a1), a2);
+    const float2 inv = make_float2(rcp_approx(sum.x), rcp_approx(sum.y));
+    const float2 w0 = __fmul2_rn(a0, inv), w1 = __fmul2_rn(a1, inv), w2 = __fmul2_rn(a2, inv);
+    // integer-coefficient stencils (coefficients summing to exactly 6), then 1/6:
+    // pre-divided coefficients do not sum to 1 in float and were measured to
+    // bias the faces by the deviation's size (4x the error against FP64)
+    const float2 p0 = __fmul2_rn(__ffma2_rn(c(11.f), f2, __ffma2_rn(c(-7.f), f1, __fmul2_rn(c(2.f), f0))),
+                                 c(1.f / 6.f));
+    const float2 p1 = __fmul2_rn(__ffma2_rn(c(2.f), f3, __ffma2_rn(c(5.f), f2, __fmul2_rn(c(-1.f), f1))),
+                                 c(1.f / 6.f));
+    const float2 p2 = __fmul2_rn(__ffma2_rn(c(-1.f), f4, __ffma2_rn(c(5.f), f3, __fmul2_rn(c(2.f), f2))),
+                                 c(1.f / 6.f));
+    return __ffma2_rn(w2, p2, __ffma2_rn(w1, p1, __fmul2_rn(w0, p0)));
+}
+
+// The 10 WENO5 reconstructions of one face in the FP32 form, paired as
+// (plus q0, plus q1), (plus q2, plus q3), (minus q0, minus q1), (minus q2,
+// minus q3) and (plus q4, minus q4). P(m, q) / M(m, q): the plus / minus
+// window value (minus already reversed) at position m of component q.
+template <class GP, class GM>
+__device__ __forceinline__ void weno5_face_x2(GP P, GM M, float face[5]) {
+    auto pr = [](float x, float y) { return make_float2(x, y); };
+    const float2 p01 = weno5x2(pr(P(0, 0), P(0, 1)), pr(P(1, 0), P(1, 1)), pr(P(2, 0), P(2, 1)),
+                               pr(P(3, 0), P(3, 1)), pr(P(4, 0), P(4, 1)));
+    const float2 p23 = weno5x2(pr(P(0, 2), P(0, 3)), pr(P(1, 2), P(1, 3)), pr(P(2, 2), P(2, 3)),
+                               pr(P(3, 2), P(3, 3)), pr(P(4, 2), P(4, 3)));
+    const float2 m01 = weno5x2(pr(M(0, 0), M(0, 1)), pr(M(1, 0), M(1, 1)), pr(M(2, 0), M(2, 1)),
+                               pr(M(3, 0), M(3, 1)), pr(M(4, 0), M(4, 1)));
+    const float2 m23 = weno5x2(pr(M(0, 2), M(0, 3)), pr(M(1, 2), M(1, 3)), pr(M(2, 2), M(2, 3)),
+                               pr(M(3, 2), M(3, 3)), pr(M(4, 2), M(4, 3)));
+    const float2 pm4 = weno5x2(pr(P(0, 4), M(0, 4)), pr(P(1, 4), M(1, 4)), pr(P(2, 4), M(2, 4)),
+                               pr(P(3, 4), M(3, 4)), pr(P(4, 4), M(4, 4)));
+    face[0] = p01.x + m01.x;
+    face[1] = p01.y + m01.y;
+    face[2] = p23.x + m23.x;
+    face[3] = p23.y + m23.y;
+    face[4] = pm4.x + pm4.y;
+}
+
 // mdcd_hybrid_reconstruction (reconstruction.cpp:151-225).
 template <class R>
 __device__ __forceinline__ R mdcd_hybrid(const R* s, const R* lin6, R disp, R diss) {

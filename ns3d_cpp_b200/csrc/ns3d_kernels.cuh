@@ -184,17 +184,23 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
         }
         split_raw(cur, fp[S - 1], fm[S - 1], false);
         R face[5];
+        if constexpr (kDeviation && RC == RC_WENO5) {
+            // reconstruct_select reverses the minus window (flag < 0)
+            weno5_face_x2([&](int m, int q) { return fp[m][q]; },
+                          [&](int m, int q) { return fm[S - 1 - m][q]; }, face);
+        } else {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            R a[S], b[S];
+            for (int q = 0; q < 5; ++q) {
+                R a[S], b[S];
 #pragma unroll
-            for (int m = 0; m < S; ++m) {
-                a[m] = fp[m][q];
-                b[m] = fm[S - 1 - m][q];  // reconstruct_select reverses for flag < 0
+                for (int m = 0; m < S; ++m) {
+                    a[m] = fp[m][q];
+                    b[m] = fm[S - 1 - m][q];  // reconstruct_select reverses for flag < 0
+                }
+                const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+                const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+                face[q] = plus_face + minus_face;
             }
-            const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
-            const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
-            face[q] = plus_face + minus_face;
         }
         if (t > 0) {
 #pragma unroll
@@ -309,6 +315,15 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     // face at chunk-relative position `pos` (face pos sits between cells pos and
     // pos+1 of the chunk in slot `cs`); window cells pos-MID .. pos-MID+S-1
     auto face_at = [&](int cs, int pos, R* face) {
+        if constexpr (kDeviation && RC == RC_WENO5) {
+            auto at = [&](int m) {
+                int k = cs * 32 + pos - MID + m;
+                return k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
+            };
+            weno5_face_x2([&](int m, int q) { return rp[q][at(m)]; },
+                          [&](int m, int q) { return rm[q][at(S - 1 - m)]; }, face);
+            return;
+        }
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             R a[S], b[S];
