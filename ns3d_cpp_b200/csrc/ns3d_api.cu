@@ -42,7 +42,7 @@ struct ns3d_ctx {
     double* wmem = nullptr;      // 3 state buffers x 6 arrays x n
     int cur = 0, rec = 0;        // current state buffer, recorded (U0) buffer
     void* tacc = nullptr;        // 5 n (R)
-    void* fv = nullptr;          // 9 n (R)
+    void* fv = nullptr;          // viscous fluxes: 9 n doubles (FP64) or 3 n float4 (FP32)
     size_t rsize = 8;            // sizeof(R)
     Ctrl* ctrl = nullptr;
     Ctrl* ctrl_host = nullptr;   // pinned mirror
@@ -580,7 +580,7 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
     const size_t n = (size_t)ctx->n;
     if (cudaMalloc(&ctx->wmem, sizeof(double) * 18 * n) != cudaSuccess ||
         cudaMalloc(&ctx->tacc, ctx->rsize * 5 * n) != cudaSuccess ||
-        cudaMalloc(&ctx->fv, ctx->rsize * 9 * n) != cudaSuccess ||
+        cudaMalloc(&ctx->fv, ctx->rsize * (ctx->rsize == 4 ? fv_values_per_cell<float>() : fv_values_per_cell<double>()) * n) != cudaSuccess ||
         cudaMalloc(&ctx->ctrl, sizeof(Ctrl)) != cudaSuccess) {
         cudaGetLastError();
         return bail(NS3D_ERR_NOMEM, "device allocation failed");

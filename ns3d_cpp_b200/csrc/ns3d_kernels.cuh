@@ -392,11 +392,42 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
 }
 
 // ---------------------------------------------------------------------------
+// Viscous flux storage (fv). FP64 form: 9 blocks of n in the order 0 xx, 1 yy,
+// 2 zz, 3 xy, 4 xz, 5 yz, 6 ex, 7 ey, 8 ez. FP32 form: three float4 blocks of
+// n, one per direction compute_vis_flux differentiates,
+//   X = (xx, xy, xz, ex) (Fv), Y = (xy, yy, yz, ey) (Hv), Z = (xz, yz, zz, ez) (Gv),
+// so the update reads the four values of one stencil offset with one 16-byte
+// load (24 loads per cell instead of 96) for 12 floats stored instead of 9.
+// ---------------------------------------------------------------------------
+template <class R>
+constexpr int fv_values_per_cell() { return sizeof(R) == 4 ? 12 : 9; }
+
+template <class R>
+__device__ __forceinline__ void store_fv(R* fv, long long n, long long id, R txx, R tyy, R tzz,
+                                         R txy, R txz, R tyz, R ex, R ey, R ez) {
+    if constexpr (sizeof(R) == 4) {
+        float4* F = reinterpret_cast<float4*>(fv);
+        F[id] = make_float4(txx, txy, txz, ex);
+        F[n + id] = make_float4(txy, tyy, tyz, ey);
+        F[2 * n + id] = make_float4(txz, tyz, tzz, ez);
+    } else {
+        fv[0 * n + id] = txx;
+        fv[1 * n + id] = tyy;
+        fv[2 * n + id] = tzz;
+        fv[3 * n + id] = txy;
+        fv[4 * n + id] = txz;
+        fv[5 * n + id] = tyz;
+        fv[6 * n + id] = ex;
+        fv[7 * n + id] = ey;
+        fv[8 * n + id] = ez;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Viscous flux (compute_gradients ViscousFlux.cpp:240-279 +
-// compute_viscous_flux :282-339). Output fv (type R), 9 blocks of n:
-//   0 tau_xx, 1 tau_yy, 2 tau_zz, 3 tau_xy, 4 tau_xz, 5 tau_yz,
-//   6 E-flux x, 7 E-flux y, 8 E-flux z.
-// The reference's 12 flux arrays map onto these (Fv = {xx, xy, xz, ex},
+// compute_viscous_flux :282-339). Output fv (type R) in the layout of store_fv:
+// the stresses tau_xx..tau_yz and the energy fluxes ex, ey, ez. The
+// reference's 12 flux arrays map onto these (Fv = {xx, xy, xz, ex},
 // Hv = {xy, yy, yz, ey}, Gv = {xz, yz, zz, ez}); the mass fluxes are zero.
 // ---------------------------------------------------------------------------
 template <class R, int ORD>
@@ -453,15 +484,9 @@ k_visc_flux(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict
     const R qy = mu * Cp / Pr * dT_dy;
     const R qz = mu * Cp / Pr * dT_dz;
     const R u = R(W.u[id]), v = R(W.v[id]), w = R(W.w[id]);
-    fv[0 * n + id] = tau_xx;
-    fv[1 * n + id] = tau_yy;
-    fv[2 * n + id] = tau_zz;
-    fv[3 * n + id] = tau_xy;
-    fv[4 * n + id] = tau_xz;
-    fv[5 * n + id] = tau_yz;
-    fv[6 * n + id] = u * tau_xx + v * tau_xy + w * tau_xz + qx;
-    fv[7 * n + id] = u * tau_xy + v * tau_yy + w * tau_yz + qy;
-    fv[8 * n + id] = u * tau_xz + v * tau_yz + w * tau_zz + qz;
+    store_fv<R>(fv, n, id, tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz,
+                u * tau_xx + v * tau_xy + w * tau_xz + qx, u * tau_xy + v * tau_yy + w * tau_yz + qy,
+                u * tau_xz + v * tau_yz + w * tau_zz + qz);
 }
 
 // ---------------------------------------------------------------------------
@@ -475,8 +500,10 @@ k_visc_flux(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict
 constexpr int VT_X = 32, VT_Y = 8, VT_H = 4;
 constexpr int VT_SX = VT_X + 2 * VT_H, VT_SY = VT_Y + 2 * VT_H;
 
+// (FP32: at most 64 registers, 4 blocks of 256 threads per SM; 68 registers
+// and 3 blocks measured 14% slower. FP64: 128 registers, 2 blocks.)
 template <class R, int ORD>
-__global__ void __launch_bounds__(VT_X * VT_Y)
+__global__ void __launch_bounds__(VT_X * VT_Y, sizeof(R) == 4 ? 4 : 2)
 k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict__ ctrl,
                 int zb) {
     if (ctrl && ctrl->stop) return;
@@ -548,15 +575,10 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
         const R qz = mu * Cp / Pr * dT_dz;
         const R u = R(ref[0]) + q[0][4], v = R(ref[1]) + q[1][4], w = R(ref[2]) + q[2][4];
         const long long id = plane + col;
-        fv[0 * n + id] = tau_xx;
-        fv[1 * n + id] = tau_yy;
-        fv[2 * n + id] = tau_zz;
-        fv[3 * n + id] = tau_xy;
-        fv[4 * n + id] = tau_xz;
-        fv[5 * n + id] = tau_yz;
-        fv[6 * n + id] = u * tau_xx + v * tau_xy + w * tau_xz + qx;
-        fv[7 * n + id] = u * tau_xy + v * tau_yy + w * tau_yz + qy;
-        fv[8 * n + id] = u * tau_xz + v * tau_yz + w * tau_zz + qz;
+        store_fv<R>(fv, n, id, tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz,
+                    u * tau_xx + v * tau_xy + w * tau_xz + qx,
+                    u * tau_xy + v * tau_yy + w * tau_yz + qy,
+                    u * tau_xz + v * tau_yz + w * tau_zz + qz);
 #pragma unroll
         for (int v2 = 0; v2 < 4; ++v2)
 #pragma unroll
@@ -573,28 +595,53 @@ __device__ __forceinline__ void cell_rhs(const DevParams& P, const R* __restrict
                                          long long id, R r[5]) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const long long n = P.n, sxy = (long long)nx * ny;
-    auto gx = [&](int a) {
-        return [=](int o) { return fv[a * n + id + (wrap1(i + o, nx) - i)]; };
-    };
-    auto gy = [&](int a) {
-        return [=](int o) { return fv[a * n + id + (long long)(wrap1(j + o, ny) - j) * nx]; };
-    };
-    auto gz = [&](int a) {
-        return [=](int o) { return fv[a * n + id + (long long)(wrap1(k + o, nz) - k) * sxy]; };
-    };
     const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
-    // flux blocks: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz, 6 ex, 7 ey, 8 ez
-    constexpr int FX[4] = {0, 3, 4, 6};  // Fv_momx, Fv_momy, Fv_momz, Fv_E
-    constexpr int FY[4] = {3, 1, 5, 7};  // Hv_*
-    constexpr int FZ[4] = {4, 5, 2, 8};  // Gv_*
     r[0] = R(0.0);
+    if constexpr (sizeof(R) == 4) {
+        // three float4 blocks: one 16-byte load per stencil offset and direction
+        constexpr int H = ORD / 2;
+        const float4* X = reinterpret_cast<const float4*>(fv);
+        const float4* Y = X + n;
+        const float4* Z = Y + n;
+        float4 vx[2 * H + 1], vy[2 * H + 1], vz[2 * H + 1];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        R acc = R(0.0);
-        acc += dcentral<R, ORD>(gx(FX[m]), dx);
-        acc += dcentral<R, ORD>(gy(FY[m]), dy);
-        acc += dcentral<R, ORD>(gz(FZ[m]), dz);
-        r[m + 1] = acc;
+        for (int o = -H; o <= H; ++o) {
+            if (o == 0) continue;
+            vx[o + H] = X[id + (wrap1(i + o, nx) - i)];
+            vy[o + H] = Y[id + (long long)(wrap1(j + o, ny) - j) * nx];
+            vz[o + H] = Z[id + (long long)(wrap1(k + o, nz) - k) * sxy];
+        }
+        auto comp = [](const float4& a, int m) { return m == 0 ? a.x : (m == 1 ? a.y : (m == 2 ? a.z : a.w)); };
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            R acc = R(0.0);
+            acc += dcentral<R, ORD>([&](int o) { return comp(vx[o + H], m); }, dx);
+            acc += dcentral<R, ORD>([&](int o) { return comp(vy[o + H], m); }, dy);
+            acc += dcentral<R, ORD>([&](int o) { return comp(vz[o + H], m); }, dz);
+            r[m + 1] = acc;
+        }
+    } else {
+        auto gx = [&](int a) {
+            return [=](int o) { return fv[a * n + id + (wrap1(i + o, nx) - i)]; };
+        };
+        auto gy = [&](int a) {
+            return [=](int o) { return fv[a * n + id + (long long)(wrap1(j + o, ny) - j) * nx]; };
+        };
+        auto gz = [&](int a) {
+            return [=](int o) { return fv[a * n + id + (long long)(wrap1(k + o, nz) - k) * sxy]; };
+        };
+        // flux blocks: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz, 6 ex, 7 ey, 8 ez
+        constexpr int FX[4] = {0, 3, 4, 6};  // Fv_momx, Fv_momy, Fv_momz, Fv_E
+        constexpr int FY[4] = {3, 1, 5, 7};  // Hv_*
+        constexpr int FZ[4] = {4, 5, 2, 8};  // Gv_*
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            R acc = R(0.0);
+            acc += dcentral<R, ORD>(gx(FX[m]), dx);
+            acc += dcentral<R, ORD>(gy(FY[m]), dy);
+            acc += dcentral<R, ORD>(gz(FZ[m]), dz);
+            r[m + 1] = acc;
+        }
     }
 #pragma unroll
     for (int q = 0; q < 5; ++q) r[q] += -tacc[q * n + id];
@@ -779,83 +826,6 @@ k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
         R r[5];
         cell_rhs<R, ORD>(P, tacc, fv, i, j, k, id, r);
         stage_cell<R, STAGE>(P, Wc, W0, id, r, ctrl->dt, Wn, ctrl, cand);
-    }
-    if (STAGE == 3) block_min_to(cand, &ctrl->dtmin_bits);
-}
-
-// 2.5-D form of k_update (see k_visc_flux_25d): x derivatives of the Fv set
-// and y derivatives of the Hv set from shared plane tiles, z derivatives of the
-// Gv set from register queues; then the same per-cell stage update. Measured
-// slower than k_update at 256^3 (FP32 1.11 vs 0.83 ms, FP64 2.27 vs 1.80 ms:
-// the serial plane march leaves the per-cell conversions latency-bound), so
-// it is off by default; NS3D_TILED=3 selects it for comparison.
-template <class R, int ORD, int STAGE>
-__global__ void __launch_bounds__(VT_X * VT_Y)
-k_update_25d(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
-             const R* __restrict__ fv, StateOut Wn, Ctrl* ctrl, int zb) {
-    if (ctrl->stop) return;
-    __shared__ R tf[4][VT_Y][VT_SX];  // Fv set, x halo
-    __shared__ R th[4][VT_SY][VT_X];  // Hv set, y halo
-    const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const long long n = P.n, sxy = (long long)nx * ny;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * VT_X + tx;
-    const int i0 = blockIdx.x * VT_X, j0 = blockIdx.y * VT_Y;
-    const int i = i0 + tx, j = j0 + ty;
-    const int k0 = blockIdx.z * zb, k1 = min(k0 + zb, nz);
-    // flux blocks: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz, 6 ex, 7 ey, 8 ez
-    constexpr int FX[4] = {0, 3, 4, 6};
-    constexpr int FY[4] = {3, 1, 5, 7};
-    constexpr int FZ[4] = {4, 5, 2, 8};
-    const long long col = (long long)j * nx + i;
-    R q[4][9];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const long long off = (long long)wrap1(k0 - 4 + m, nz) * sxy + col;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) q[v][m] = fv[FZ[v] * n + off];
-    }
-    const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
-    const double dt = ctrl->dt;
-    double cand = CFL_INIT;
-    for (int k = k0; k < k1; ++k) {
-        const long long plane = (long long)k * sxy;
-        {
-            const long long off = (long long)wrap1(k + 4, nz) * sxy + col;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) q[v][8] = fv[FZ[v] * n + off];
-        }
-        for (int t = tid; t < VT_Y * VT_SX; t += VT_X * VT_Y) {
-            const int ly = t / VT_SX, lx = t - ly * VT_SX;
-            const long long off = plane + (long long)(j0 + ly) * nx + wrap1(i0 - VT_H + lx, nx);
-#pragma unroll
-            for (int v = 0; v < 4; ++v) tf[v][ly][lx] = fv[FX[v] * n + off];
-        }
-        for (int t = tid; t < VT_SY * VT_X; t += VT_X * VT_Y) {
-            const int ly = t / VT_X, lx = t - ly * VT_X;
-            const long long off = plane + (long long)wrap1(j0 - VT_H + ly, ny) * nx + (i0 + lx);
-#pragma unroll
-            for (int v = 0; v < 4; ++v) th[v][ly][lx] = fv[FY[v] * n + off];
-        }
-        __syncthreads();
-        const long long id = plane + col;
-        R r[5];
-        r[0] = R(0.0);
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            R acc = R(0.0);
-            acc += dcentral<R, ORD>([&](int o) { return tf[m][ty][tx + VT_H + o]; }, dx);
-            acc += dcentral<R, ORD>([&](int o) { return th[m][ty + VT_H + o][tx]; }, dy);
-            acc += dcentral<R, ORD>([&](int o) { return q[m][4 + o]; }, dz);
-            r[m + 1] = acc;
-        }
-#pragma unroll
-        for (int qq = 0; qq < 5; ++qq) r[qq] += -tacc[qq * n + id];
-        stage_cell<R, STAGE>(P, Wc, W0, id, r, dt, Wn, ctrl, cand);
-#pragma unroll
-        for (int v2 = 0; v2 < 4; ++v2)
-#pragma unroll
-            for (int m = 0; m < 8; ++m) q[v2][m] = q[v2][m + 1];
-        __syncthreads();
     }
     if (STAGE == 3) block_min_to(cand, &ctrl->dtmin_bits);
 }

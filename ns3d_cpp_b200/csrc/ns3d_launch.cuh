@@ -16,7 +16,7 @@ struct LaunchCfg {
     int seg[3];   // cells per thread segment along x, y, z
     cudaStream_t stream;
     int zb;       // planes per block of the 2.5-D viscous kernels (0: from the grid)
-    int tiled;    // bit 0: 2.5-D visc_flux, bit 1: 2.5-D update (when the box tiles)
+    int tiled;    // bit 0: 2.5-D visc_flux (when the box tiles)
 };
 
 // Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED / NS3D_SEG for tuning.
@@ -144,13 +144,6 @@ cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl*
 template <class R, int ORD>
 static cudaError_t update_ord(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
                               const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl) {
-    if (detail::tiles_25d(L, 2)) {
-        const dim3 g = detail::grid_25d(L), b(VT_X, VT_Y);
-        if (stage == 1) k_update_25d<R, ORD, 1><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, detail::zb_for(L));
-        else if (stage == 2) k_update_25d<R, ORD, 2><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, detail::zb_for(L));
-        else k_update_25d<R, ORD, 3><<<g, b, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl, detail::zb_for(L));
-        return cudaGetLastError();
-    }
     const int th = detail::threads_for(L.P.nx);
     const dim3 g = detail::cell_grid(L.P, th);
     if (stage == 1) k_update<R, ORD, 1><<<g, th, 0, L.stream>>>(L.P, Wc, W0, tacc, fv, Wn, ctrl);

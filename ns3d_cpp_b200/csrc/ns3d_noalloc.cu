@@ -10,8 +10,8 @@
 // input and output buffers; the intermediate arrays of the RHS live in a
 // fixed-size array of this library's own device memory.
 //
-// The scratch (temperature + the inviscid accumulator + the nine viscous
-// fluxes) is the file-scope array below: 15 doubles per cell for at most
+// The scratch (temperature + the inviscid accumulator + the viscous fluxes)
+// is the file-scope array below: 15 doubles per cell for at most
 // NS3D_NOALLOC_MAX_CELLS cells, 7.5 MiB, held on every GPU that loads the
 // library until the process exits. Every call shares it and it keeps the last
 // call's contents; each kernel overwrites what it reads later in the same
@@ -19,6 +19,7 @@
 // streams, other threads) race on it and must be serialised by the caller.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -36,8 +37,8 @@ extern template cudaError_t launch_visc_flux<float>(const LaunchCfg&, StateView,
 extern template cudaError_t launch_rhs_out<float>(const LaunchCfg&, const float*, const float*, double*);
 }  // namespace ns3d
 
-// 15 values per cell: T (double) + 5 accumulator + 9 viscous-flux values
-// (double in the FP64 form, float in the FP32-stencil form).
+// 15 doubles per cell: T (double) + 5 accumulator values + the viscous fluxes
+// (9 doubles in the FP64 form; 5 + 12 floats in the FP32-stencil form).
 static __device__ __align__(256) double g_noalloc_scratch[15 * (long long)NS3D_NOALLOC_MAX_CELLS];
 
 namespace {
@@ -87,7 +88,9 @@ template <class R>
 cudaError_t rhs_into(const LaunchCfg& L, StateView W, double* scratch, double* rhs) {
     const long long n = L.P.n;
     R* tacc = reinterpret_cast<R*>(scratch + n);
-    R* fv = tacc + 5 * n;
+    // fv on a 16-byte boundary (the FP32 form reads it as float4); FP32 needs
+    // 8 + 20 + 48 bytes per cell (+12 of padding) of the 120 the array holds
+    R* fv = reinterpret_cast<R*>((reinterpret_cast<uintptr_t>(tacc + 5 * n) + 15) & ~uintptr_t(15));
     cudaError_t e = cudaSuccess;
     for (int dir = 0; dir < 3 && e == cudaSuccess; ++dir) e = launch_sweep<R>(L, dir, W, tacc, nullptr);
     if (e == cudaSuccess) e = launch_visc_flux<R>(L, W, fv, nullptr);
