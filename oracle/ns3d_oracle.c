@@ -48,6 +48,8 @@ typedef struct orc_params {
     int fvs, recon, vis;
     int mu_variant;              /* 0: pow(T, 1.5) as the reference; 1: T*sqrt(T) (a
                                     1-ulp perturbation, for sensitivity controls) */
+    int char_recon;              /* 1: characteristic-wise reconstruction
+                                    (du_inviscous_character, InviscousFlux_new.cpp:165-437) */
 } orc_params;
 
 #define IDX(i, j, k) (((long)(k) * ny + (j)) * nx + (i))
@@ -326,6 +328,52 @@ double orc_recon_scalar(const orc_params *P, const double *win, int S, double fl
 /* Inviscid face fluxes: du_inviscous, InviscousFlux_new.cpp:4-163           */
 /* ------------------------------------------------------------------------ */
 
+/* Roe-averaged state (rho, u, v, w, H) of two primitive states
+ * (computeRoeAveragedState_new, InviscousFlux_new.cpp:628-659), same operation order. */
+static void roe_state(const orc_params *P, const double *l, const double *r, double *ua) {
+    const double g = P->gamma;
+    const double EL = l[0] * (0.5 * (l[1] * l[1] + l[2] * l[2] + l[3] * l[3]) + l[4] / ((g - 1.0) * l[0]));
+    const double ER = r[0] * (0.5 * (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]) + r[4] / ((g - 1.0) * r[0]));
+    const double sl = sqrt(l[0]), sr = sqrt(r[0]);
+    ua[0] = sl * sr;
+    const double den = 1.0 / (sl + sr);
+    ua[1] = (sl * l[1] + sr * r[1]) * den;
+    ua[2] = (sl * l[2] + sr * r[2]) * den;
+    ua[3] = (sl * l[3] + sr * r[3]) * den;
+    const double HL = (EL + l[4]) / l[0];
+    const double HR = (ER + r[4]) / r[0];
+    ua[4] = (sl * HL + sr * HR) * den;
+}
+
+/* Left and right eigenvector matrices of the Euler flux Jacobian along the
+ * unit normal (nx, ny, nz) at the Roe state (build_eigen_matrices_new,
+ * InviscousFlux_new.cpp:532-625): same entries, same operation order. */
+static void eigen_LR(const orc_params *P, const double *ua, double nx, double ny, double nz,
+                     double Lm[5][5], double Rm[5][5]) {
+    const double g = P->gamma;
+    const double u0 = ua[1], v0 = ua[2], w0 = ua[3], h0 = ua[4];
+    const double V = 0.5 * (u0 * u0 + v0 * v0 + w0 * w0);
+    const double un = u0 * nx + v0 * ny + w0 * nz;
+    const double c = sqrt((g - 1.0) * (h0 - V));
+    const double t2 = u0 * nz + v0 * nx + w0 * ny;   /* the two transverse velocities */
+    const double t3 = u0 * ny + v0 * nz + w0 * nx;
+    Rm[0][0] = 1.0;          Rm[0][1] = 1.0; Rm[0][2] = 0.0; Rm[0][3] = 0.0; Rm[0][4] = 1.0;
+    Rm[1][0] = u0 - c * nx;  Rm[1][1] = u0;  Rm[1][2] = nz;  Rm[1][3] = ny;  Rm[1][4] = u0 + c * nx;
+    Rm[2][0] = v0 - c * ny;  Rm[2][1] = v0;  Rm[2][2] = nx;  Rm[2][3] = nz;  Rm[2][4] = v0 + c * ny;
+    Rm[3][0] = w0 - c * nz;  Rm[3][1] = w0;  Rm[3][2] = ny;  Rm[3][3] = nx;  Rm[3][4] = w0 + c * nz;
+    Rm[4][0] = h0 - un * c;  Rm[4][1] = V;   Rm[4][2] = t2;  Rm[4][3] = t3;  Rm[4][4] = h0 + un * c;
+    const double chi = 0.5 / c;
+    const double K = (g - 1.0) / (c * c);
+    const double K1 = K / 2;
+    Lm[0][0] = K1 * V + chi * un;  Lm[0][1] = -chi * nx - K1 * u0;  Lm[0][2] = -chi * ny - K1 * v0;
+    Lm[0][3] = -chi * nz - K1 * w0;  Lm[0][4] = K1;
+    Lm[1][0] = 1.0 - K * V;  Lm[1][1] = K * u0;  Lm[1][2] = K * v0;  Lm[1][3] = K * w0;  Lm[1][4] = -K;
+    Lm[2][0] = -t2;  Lm[2][1] = nz;  Lm[2][2] = nx;  Lm[2][3] = ny;  Lm[2][4] = 0.0;
+    Lm[3][0] = -t3;  Lm[3][1] = ny;  Lm[3][2] = nz;  Lm[3][3] = nx;  Lm[3][4] = 0.0;
+    Lm[4][0] = K1 * V - chi * un;  Lm[4][1] = chi * nx - K1 * u0;  Lm[4][2] = chi * ny - K1 * v0;
+    Lm[4][3] = chi * nz - K1 * w0;  Lm[4][4] = K1;
+}
+
 /* Face fluxes of direction `dir` (0=x,1=y,2=z) for every line. Output F has
  * 5 blocks of n; F[q*n + idx(cell)] is the flux through the face on the +side
  * of that cell (face i+1/2 for dir x), i.e. the reference's flux_f? at index
@@ -371,6 +419,41 @@ void orc_face_fluxes(const orc_params *P, const double *W, int dir, double *Fout
                     int i = dir == 0 ? f : a, j = dir == 1 ? f : (dir == 0 ? a : b),
                         k = dir == 2 ? f : b;
                     long id = IDX(i, j, k);
+                    if (P->char_recon) {
+                        /* du_inviscous_character: Roe state of the face's two cells,
+                         * windows projected on the left eigenvectors, one
+                         * reconstruction per characteristic field, back by R. */
+                        const int f1 = wrap(f + 1, len);
+                        const long idr = IDX(dir == 0 ? f1 : i, dir == 1 ? f1 : j, dir == 2 ? f1 : k);
+                        double wl[5], wr[5], ua[5], Lm[5][5], Rm[5][5], wc[5];
+                        for (int q = 0; q < 5; ++q) {
+                            wl[q] = W[q * n + id];
+                            wr[q] = W[q * n + idr];
+                        }
+                        roe_state(P, wl, wr, ua);
+                        eigen_LR(P, ua, (double)n1, (double)n2, (double)n3, Lm, Rm);
+                        for (int q = 0; q < 5; ++q) {
+                            double wp[8], wm[8];
+                            for (int m = 0; m < S; ++m) {
+                                const double *fp = &Fp[5 * (f + (m - mid) + S)];
+                                const double *fm = &Fm[5 * (f + (m - mid) + S)];
+                                double sp = 0.0, sm = 0.0;
+                                for (int r = 0; r < 5; ++r) {
+                                    sp += Lm[q][r] * fp[r];
+                                    sm += Lm[q][r] * fm[r];
+                                }
+                                wp[m] = sp;
+                                wm[m] = sm;
+                            }
+                            wc[q] = recon_select(P, wp, S, +1.0) + recon_select(P, wm, S, -1.0);
+                        }
+                        for (int q = 0; q < 5; ++q) {
+                            double sum = 0.0;
+                            for (int r = 0; r < 5; ++r) sum += Rm[q][r] * wc[r];
+                            Fout[q * n + id] = sum;
+                        }
+                        continue;
+                    }
                     for (int q = 0; q < 5; ++q) {
                         double wp[8], wm[8];
                         for (int m = 0; m < S; ++m) {

@@ -84,7 +84,9 @@ def derived(cfg: dict) -> dict:
                 ud7l_alpha=float(cfg.get("ud7l_alpha", 0.4)),
                 cfl=float(cfg.get("cfl", 0.1)), dt_fixed=float(cfg.get("dt_fixed", -1.0)),
                 sw_eps=float(cfg.get("sw_entropy_eps", 0.0)),
-                sutherland_s=float(cfg.get("sutherland_s_over_tref", SUTHERLAND_REF)))
+                sutherland_s=float(cfg.get("sutherland_s_over_tref", SUTHERLAND_REF)),
+                # initialization.cpp:260-261 (values lower-cased before the test)
+                char_recon=int(str(cfg.get("char_recon", "false")).lower() in ("yes", "true")))
 
 
 # --------------------------------------------------------------------------
@@ -95,7 +97,8 @@ class OrcParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ("gamma", "Pr", "Ma", "Re", "Cv", "Cp", "Rgas", "mu", "dx", "dy", "dz",
                  "mdcd_diss", "mdcd_disp", "ud7l_alpha", "sw_eps", "sutherland_s")] + \
-              [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "fvs", "recon", "vis", "mu_variant")]
+              [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "fvs", "recon", "vis", "mu_variant",
+                                           "char_recon")]
 
 
 def _dp(a: np.ndarray):

@@ -64,6 +64,17 @@ SCHEMES = [
 ]
 
 
+# characteristic-wise reconstruction (du_inviscous_character) over the
+# splittings and reconstruction families
+CHAR_SCHEMES = [
+    dict(char_recon="true"),
+    dict(char_recon="true", fvs_type="LaxFriedrichs", recon="MDCD"),
+    dict(char_recon="true", recon="UPWIND_7TH", vis_scheme="C4th"),
+    dict(char_recon="true", recon="MDCD_HYBRID", vis_scheme="C6th"),
+    dict(char_recon="true", fvs_type="LaxFriedrichs", recon="LINEAR"),
+]
+
+
 def scheme_id(kw):
     return "-".join(f"{k}={v}" for k, v in kw.items()) or "default"
 

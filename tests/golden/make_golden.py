@@ -20,7 +20,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-from conftest import SCHEMES, ref_cfg, scheme_id  # noqa: E402
+from conftest import CHAR_SCHEMES, SCHEMES, ref_cfg, scheme_id  # noqa: E402
 
 
 def golden_input(n: int, Ma: float = 0.1, gamma: float = 1.4) -> np.ndarray:
@@ -54,7 +54,7 @@ def main():
     if not oracle.have_ref():
         oracle.build(ref=True)
     out = {}
-    for kw in SCHEMES:
+    for kw in SCHEMES + CHAR_SCHEMES:
         n = 8
         cfg = ref_cfg(n, **kw)
         r = oracle.Ref(cfg)

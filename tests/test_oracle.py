@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 from numpy.polynomial import polynomial as Pn
 
-from conftest import SCHEMES, ref_cfg, relerr, scheme_id
+from conftest import CHAR_SCHEMES, SCHEMES, ref_cfg, relerr, scheme_id
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -19,7 +19,7 @@ def golden_input(n):
     return gi(n)
 
 
-@pytest.mark.parametrize("kw", SCHEMES, ids=scheme_id)
+@pytest.mark.parametrize("kw", SCHEMES + CHAR_SCHEMES, ids=scheme_id)
 def test_oracle_matches_reference_golden(oracle_mod, kw):
     """RHS and two CFL steps of the oracle equal the reference's outputs."""
     g = np.load(os.path.join(GOLD, "rhs_steps_8.npz"))
@@ -68,6 +68,31 @@ def test_oracle_bit_exact_vs_live_reference(oracle_mod, kw):
     r.set_primitive(W)
     o = oracle_mod.Oracle(cfg)
     assert np.array_equal(o.rhs(W), r.rhs())
+    Wo = W
+    for _ in range(3):
+        dtr = r.cfl_step()
+        Wo, dto, st = o.cfl_step(Wo)
+        assert dtr == dto and st == 0
+    assert np.array_equal(Wo, r.W())
+
+
+@needs_ref
+@pytest.mark.parametrize("kw", CHAR_SCHEMES, ids=scheme_id)
+def test_oracle_char_recon_bit_exact_vs_live_reference(oracle_mod, kw):
+    """Characteristic-wise reconstruction (du_inviscous_character): bit-exact
+    RHS and 3 CFL steps against the reference on a non-power-of-two box."""
+    from ns3d_cpp_b200 import initial
+    n = 12
+    cfg = ref_cfg(n, **kw)
+    W = initial.taylor_green(n, Ma=0.1, perturb=0.05, seed=7)
+    r = oracle_mod.Ref(cfg)
+    r.set_primitive(W)
+    o = oracle_mod.Oracle(cfg)
+    rhs = o.rhs(W)
+    assert np.array_equal(rhs, r.rhs())
+    # the characteristic path differs from the component-wise one
+    assert not np.array_equal(rhs, oracle_mod.Oracle(ref_cfg(n, **{k: v for k, v in kw.items()
+                                                                  if k != "char_recon"})).rhs(W))
     Wo = W
     for _ in range(3):
         dtr = r.cfl_step()
