@@ -166,7 +166,14 @@ def make_params(ns, n, precision, dt_fixed=-1.0):
     return ns.SolverParams.default().replace(
         n=n, gamma=w["gamma"], Pr=w["Pr"], Ma=w["Ma"], Re=w["Re"], cfl=w["cfl"],
         dt_fixed=dt_fixed, fvs_type=w["fvs"], recon=w["recon"], vis_scheme=w["vis"],
-        Lx=two_pi, Ly=two_pi, Lz=two_pi, precision=precision)
+        Lx=two_pi, Ly=two_pi, Lz=two_pi, precision=precision,
+        char_recon=1 if w.get("char") else 0)
+
+
+def workload_name(n):
+    w = WORKLOAD
+    scheme = "SW+WENO5, C8th" + (", characteristic-wise reconstruction" if w.get("char") else "")
+    return f"isotropic turbulence {n}^3, Mach_t 0.5, Re 1000, {scheme}"
 
 
 def workload_input(n):
@@ -382,7 +389,8 @@ def our_arm(args, rank, world, local):
                          "achieved_gbs": b / (kms / cnt / 1e3) / 1e9 if b else None}
     dom = max((c for c in kern if c != "other"), key=lambda c: kern[c]["ms_total"])
     tr = ncu_traffic()
-    traffic = tr.get(f"fp32acc64/{dom}")
+    # captured traffic belongs to the component-wise kernels
+    traffic = None if WORKLOAD.get("char") else tr.get(f"fp32acc64/{dom}")
     traffic = None if traffic is None else traffic * 1e9 * (ncell / 256 ** 3)
     # algorithmic bytes of the captured launch (the update capture is a stage-2 launch)
     cap_alg = tr.get(f"fp32acc64/{dom}/alg_bytes_per_cell")
@@ -408,7 +416,7 @@ def our_arm(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 stencils / fp64 accumulate",
         "data": "synthetic: seeded isotropic turbulence (numpy), inputs resident in HBM",
-        "config": {"workload": f"isotropic turbulence {n}^3, Mach_t 0.5, Re 1000, SW+WENO5, C8th",
+        "config": {"workload": workload_name(n),
                    "n": n, "cells": ncell, "precision": "fp32acc64",
                    "l2": f"inputs larger than L2: {6 * ncell * 8 / 1e6:.0f} MB per state buffer",
                    "parallelism": f"replicas x{world}"},
@@ -437,7 +445,7 @@ def our_arm(args, rank, world, local):
 def _cpu_worker(args):
     """One replica: the reference (or the oracle port) on a periodic sub-box.
     Runs in a spawned process; returns seconds per RK3 step."""
-    kind, n, steps, warm = args
+    kind, n, steps, warm, char = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from ns3d_cpp_b200 import initial
@@ -447,7 +455,7 @@ def _cpu_worker(args):
                fvs_type="StagerWarming", recon="WENO5", vis_scheme="C8th",
                global_nx=n, global_ny=n, global_nz=n, Lx=two_pi, Ly=two_pi, Lz=two_pi,
                Post_BasicField="False", IsotropicAnalyse="False", monitor_Res="False",
-               monitor_Energy="False")
+               monitor_Energy="False", char_recon="true" if char else "false")
     W = initial.isotropic(n, mach_t=w["mach_t"], Ma=w["Ma"], gamma=w["gamma"], k0=w["k0"],
                           seed=w["seed"])
     if kind == "reference":
@@ -480,7 +488,8 @@ def run_cpu(steps: int, warm: int, n_equiv: int):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        per_step = pool.map(_cpu_worker, [(kind, CPU_SAMPLE_N, steps, warm)] * cores)
+        per_step = pool.map(_cpu_worker,
+                            [(kind, CPU_SAMPLE_N, steps, warm, bool(WORKLOAD.get("char")))] * cores)
     wall = time.perf_counter() - t0
     cells = CPU_SAMPLE_N ** 3
     cell_rate = sum(cells / t for t in per_step)
@@ -507,8 +516,7 @@ def reference_arm(args, rank, world):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded isotropic turbulence (numpy)",
-            "config": {"workload": (f"isotropic turbulence {args.n}^3, Mach_t 0.5, Re 1000, "
-                                    "SW+WENO5, C8th"), "n": args.n},
+            "config": {"workload": workload_name(args.n), "n": args.n},
             "cpu_baseline": {"value": res["value"], "unit": "steps/s", "cores": res["cores"],
                              "kind": res["kind"], "sample": res["sample"]},
             "e2e": {"value": res["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
@@ -530,8 +538,13 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true", help="only the headline form")
     ap.add_argument("--skip-adjoint", action="store_true", help="no adjoint cost measurement")
+    ap.add_argument("--char-recon", action="store_true",
+                    help="characteristic-wise reconstruction in both arms (char_recon)")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
+    if args.char_recon:
+        WORKLOAD["char"] = True
+        args.skip_adjoint = True   # the adjoint is component-wise only
     rank, world, local = env_rank()
     if args.impl == "reference":
         reference_arm(args, rank, world)

@@ -30,7 +30,7 @@ typedef enum ns3d_status {
     NS3D_OK = 0,
     NS3D_ERR_INVALID = 1,      /* bad argument or configuration */
     NS3D_ERR_UNSUPPORTED = 2,  /* valid in the reference, not built here: non-periodic
-                                  boundaries, char_recon, WCNS */
+                                  boundaries, WCNS; adjoint of MDCD_HYBRID / char_recon */
     NS3D_ERR_CUDA = 3,         /* CUDA runtime / cuFFT failure */
     NS3D_ERR_NONPHYSICAL = 4,  /* rho, p or T <= 0 after a step (range_kutta.cpp:149-162) */
     NS3D_ERR_FILE = 5,         /* solver.in cannot be opened (initialization.cpp:206-209) */
@@ -119,8 +119,9 @@ size_t ns3d_turb_stats_size(void);
 /* ---- context ------------------------------------------------------------- */
 
 /* Field3D::allocate (field_structures.h:225) on `device`, interior-only and
- * resident in HBM. Rejects non-periodic boundaries, char_recon and WCNS with
- * NS3D_ERR_UNSUPPORTED. */
+ * resident in HBM. Rejects non-periodic boundaries and WCNS with
+ * NS3D_ERR_UNSUPPORTED. char_recon selects the characteristic-wise sweeps
+ * (du_inviscous_character, InviscousFlux_new.cpp:165-437). */
 ns3d_status ns3d_create(const ns3d_params *p, int device, ns3d_ctx **out);
 ns3d_status ns3d_destroy(ns3d_ctx *ctx);
 /* Last error message of this context (static string for ctx == NULL). */
@@ -179,8 +180,9 @@ ns3d_status ns3d_last_dt(ns3d_ctx *ctx, double *dt);
 /* The derivative of exactly the FP64 forward arithmetic (the adjoint of the
  * discretisation, not of the PDE). Supported: FP64 form, Steger-Warming (use
  * sw_entropy_eps > 0 to make |lambda| smooth) or Lax-Friedrichs, WENO5 or the
- * linear reconstructions; MDCD_HYBRID returns NS3D_ERR_UNSUPPORTED. Arrays
- * are host pointers to 5 consecutive interior blocks (rho, u, v, w, p). */
+ * linear reconstructions, component-wise; MDCD_HYBRID and char_recon return
+ * NS3D_ERR_UNSUPPORTED. Arrays are host pointers to 5 consecutive interior
+ * blocks (rho, u, v, w, p). */
 
 /* lam_w = (d rhs / d w)^T lam_rhs at the current state (vector-Jacobian
  * product of compute_rhs with respect to the primitives). */

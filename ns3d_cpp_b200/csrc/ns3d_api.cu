@@ -246,10 +246,6 @@ ns3d_status validate(const ns3d_params* p, std::string& msg) {
             msg = "only periodic boundaries are built (boundary.cpp:56-207 is out of scope)";
             return NS3D_ERR_UNSUPPORTED;
         }
-    if (p->char_recon) {
-        msg = "char_recon (InviscousFlux_new.cpp:165-437) is not built";
-        return NS3D_ERR_UNSUPPORTED;
-    }
     if (recon_kind(p->recon) < 0) {
         msg = "reconstruction WCNS has no implementation in the reference either";
         return NS3D_ERR_UNSUPPORTED;
@@ -516,6 +512,7 @@ ns3d_status build_launch_cfg(const ns3d_params* p, LaunchCfg* L, std::string* ms
     P.vis_order = q.vis_scheme == NS3D_VIS_C4TH ? 4 : (q.vis_scheme == NS3D_VIS_C6TH ? 6 : 8);
     L->fvs = q.fvs_type == NS3D_FVS_STEGER_WARMING ? FV_SW : FV_LF;
     L->rc = recon_kind(q.recon);
+    L->chr = q.char_recon ? 1 : 0;
     for (int d = 0; d < 3; ++d) L->seg[d] = 0;  // chosen per launch from the grid
     default_tiling(*L);
     L->stream = nullptr;
@@ -563,6 +560,7 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
     P.vis_order = q.vis_scheme == NS3D_VIS_C4TH ? 4 : (q.vis_scheme == NS3D_VIS_C6TH ? 6 : 8);
     ctx->L.fvs = q.fvs_type == NS3D_FVS_STEGER_WARMING ? FV_SW : FV_LF;
     ctx->L.rc = recon_kind(q.recon);
+    ctx->L.chr = q.char_recon ? 1 : 0;
     for (int d = 0; d < 3; ++d) ctx->L.seg[d] = 0;  // chosen per launch from the grid
     default_tiling(ctx->L);
     ctx->rsize = q.precision == NS3D_PREC_FP64 ? sizeof(double) : sizeof(float);
@@ -893,6 +891,8 @@ ns3d_status adjoint_supported(ns3d_ctx* ctx) {
         return fail(ctx, NS3D_ERR_UNSUPPORTED, "the adjoint differentiates the FP64 form");
     if (ctx->L.rc == RC_MDCD_HYBRID)
         return fail(ctx, NS3D_ERR_UNSUPPORTED, "no adjoint for MDCD_HYBRID");
+    if (ctx->L.chr)
+        return fail(ctx, NS3D_ERR_UNSUPPORTED, "no adjoint for characteristic-wise reconstruction");
     return NS3D_OK;
 }
 

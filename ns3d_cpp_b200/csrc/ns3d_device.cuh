@@ -207,6 +207,62 @@ __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, d
 }
 
 // ---------------------------------------------------------------------------
+// Characteristic-wise reconstruction (du_inviscous_character,
+// InviscousFlux_new.cpp:165-437): at each face the Roe-averaged state of its
+// two cells, the left / right eigenvector matrices along the face normal, the
+// split-flux windows projected on the left eigenvectors, one reconstruction
+// per characteristic field, and the result mapped back by the right ones.
+// ---------------------------------------------------------------------------
+
+// computeRoeAveragedState_new (InviscousFlux_new.cpp:628-659): (rho, u, v, w, H)
+// of two primitive states (rho, u, v, w, p); same operation order.
+__device__ __forceinline__ void roe_state(double gamma, const double* l, const double* r,
+                                          double* ua) {
+    const double EL = l[0] * (0.5 * (l[1] * l[1] + l[2] * l[2] + l[3] * l[3]) +
+                              l[4] / ((gamma - 1.0) * l[0]));
+    const double ER = r[0] * (0.5 * (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]) +
+                              r[4] / ((gamma - 1.0) * r[0]));
+    const double sl = sqrt(l[0]), sr = sqrt(r[0]);
+    ua[0] = sl * sr;
+    const double den = 1.0 / (sl + sr);
+    ua[1] = (sl * l[1] + sr * r[1]) * den;
+    ua[2] = (sl * l[2] + sr * r[2]) * den;
+    ua[3] = (sl * l[3] + sr * r[3]) * den;
+    const double HL = (EL + l[4]) / l[0];
+    const double HR = (ER + r[4]) / r[0];
+    ua[4] = (sl * HL + sr * HR) * den;
+}
+
+// build_eigen_matrices_new (InviscousFlux_new.cpp:532-625) along the unit normal
+// (N1, N2, N3): the same entries in the same operation order.
+template <int N1, int N2, int N3>
+__device__ __forceinline__ void eigen_LR(double gamma, const double* ua, double Lm[5][5],
+                                         double Rm[5][5]) {
+    const double nx = N1, ny = N2, nz = N3;
+    const double u0 = ua[1], v0 = ua[2], w0 = ua[3], h0 = ua[4];
+    const double V = 0.5 * (u0 * u0 + v0 * v0 + w0 * w0);
+    const double un = u0 * nx + v0 * ny + w0 * nz;
+    const double c = sqrt((gamma - 1.0) * (h0 - V));
+    const double t2 = u0 * nz + v0 * nx + w0 * ny;  // the two transverse velocities
+    const double t3 = u0 * ny + v0 * nz + w0 * nx;
+    Rm[0][0] = 1.0;         Rm[0][1] = 1.0; Rm[0][2] = 0.0; Rm[0][3] = 0.0; Rm[0][4] = 1.0;
+    Rm[1][0] = u0 - c * nx; Rm[1][1] = u0;  Rm[1][2] = nz;  Rm[1][3] = ny;  Rm[1][4] = u0 + c * nx;
+    Rm[2][0] = v0 - c * ny; Rm[2][1] = v0;  Rm[2][2] = nx;  Rm[2][3] = nz;  Rm[2][4] = v0 + c * ny;
+    Rm[3][0] = w0 - c * nz; Rm[3][1] = w0;  Rm[3][2] = ny;  Rm[3][3] = nx;  Rm[3][4] = w0 + c * nz;
+    Rm[4][0] = h0 - un * c; Rm[4][1] = V;   Rm[4][2] = t2;  Rm[4][3] = t3;  Rm[4][4] = h0 + un * c;
+    const double chi = 0.5 / c;
+    const double K = (gamma - 1.0) / (c * c);
+    const double K1 = K / 2;
+    Lm[0][0] = K1 * V + chi * un;    Lm[0][1] = -chi * nx - K1 * u0; Lm[0][2] = -chi * ny - K1 * v0;
+    Lm[0][3] = -chi * nz - K1 * w0;  Lm[0][4] = K1;
+    Lm[1][0] = 1.0 - K * V;  Lm[1][1] = K * u0;  Lm[1][2] = K * v0;  Lm[1][3] = K * w0;  Lm[1][4] = -K;
+    Lm[2][0] = -t2;  Lm[2][1] = nz;  Lm[2][2] = nx;  Lm[2][3] = ny;  Lm[2][4] = 0.0;
+    Lm[3][0] = -t3;  Lm[3][1] = ny;  Lm[3][2] = nz;  Lm[3][3] = nx;  Lm[3][4] = 0.0;
+    Lm[4][0] = K1 * V - chi * un;    Lm[4][1] = chi * nx - K1 * u0;  Lm[4][2] = chi * ny - K1 * v0;
+    Lm[4][3] = chi * nz - K1 * w0;   Lm[4][4] = K1;
+}
+
+// ---------------------------------------------------------------------------
 // Scalar reconstructions (reconstruction.cpp). `s` is the window after the
 // reversal that reconstruct_select applies for the minus flux (:24-31).
 // ---------------------------------------------------------------------------

@@ -66,7 +66,7 @@ __device__ __forceinline__ int wrap1(int s, int len) {
 //   DIR 2: lines over (i,j), threads over i        (coalesced along x)
 // T_acc (5 blocks of n, type R): DIR 0 writes ax*idx, DIR 1 and 2 add.
 // ---------------------------------------------------------------------------
-template <int DIR, class R, int FVS, int RC>
+template <int DIR, class R, int FVS, int RC, bool CHR = false>
 __global__ void __launch_bounds__(128)
 k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
@@ -158,6 +158,47 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     };
     (void)gamma;
     (void)eps;
+    // CHR: du_inviscous_character. The face's two cells are reloaded (L1/L2
+    // hits); rho unclamped, as the reference reads F.rho. In the FP32 form the
+    // windows are deviations from the segment's offset, which the projection
+    // and reconstruction carry through unchanged (R L ref = ref cancels in the
+    // face difference).
+    auto char_face = [&](int f, R* face) {
+        double wl[5], wr[5], ua[5], Lm[5][5], Rm[5][5];
+        load_raw(f, wl);
+        load_raw(f + 1, wr);
+        roe_state(P.gamma, wl, wr, ua);
+        eigen_LR<DIR == 0, DIR == 1, DIR == 2>(P.gamma, ua, Lm, Rm);
+        R wc[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            R a[S], bc[S], b[S];
+#pragma unroll
+            for (int m = 0; m < S; ++m) {
+                R sp = R(0.0), sm = R(0.0);
+#pragma unroll
+                for (int r = 0; r < 5; ++r) {
+                    sp += R(Lm[q][r]) * fp[m][r];
+                    sm += R(Lm[q][r]) * fm[m][r];
+                }
+                a[m] = sp;
+                bc[m] = sm;
+            }
+#pragma unroll
+            for (int m = 0; m < S; ++m) b[m] = bc[S - 1 - m];
+            const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+            const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+            wc[q] = plus_face + minus_face;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            R sum = R(0.0);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) sum += R(Rm[q][r]) * wc[r];
+            face[q] = sum;
+        }
+    };
+    (void)char_face;
 
     int f = c0 - 1;  // face f sits between cells f and f+1 (the reference's i_face = f + ng)
     double nxt[5];
@@ -184,7 +225,9 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
         }
         split_raw(cur, fp[S - 1], fm[S - 1], false);
         R face[5];
-        if constexpr (kDeviation && RC == RC_WENO5) {
+        if constexpr (CHR) {
+            char_face(f, face);
+        } else if constexpr (kDeviation && RC == RC_WENO5) {
             // reconstruct_select reverses the minus window (flag < 0)
             weno5_face_x2([&](int m, int q) { return fp[m][q]; },
                           [&](int m, int q) { return fm[S - 1 - m][q]; }, face);

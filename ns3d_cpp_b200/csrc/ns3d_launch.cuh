@@ -13,6 +13,7 @@ struct LaunchCfg {
     DevParams P;
     int fvs;      // FV_SW / FV_LF
     int rc;       // RC_* of the reconstruction
+    int chr;      // 1: characteristic-wise reconstruction (char_recon)
     int seg[3];   // cells per thread segment along x, y, z
     cudaStream_t stream;
     int zb;       // planes per block of the 2.5-D viscous kernels (0: from the grid)
@@ -55,10 +56,10 @@ inline int segment_for(int len, long long lines) {
 
 namespace detail {
 
-template <int DIR, class R, int FVS, int RC>
+template <int DIR, class R, int FVS, int RC, bool CHR>
 cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl) {
     const DevParams& P = L.P;
-    if (DIR == 0 && P.nx % 32 == 0) {
+    if (DIR == 0 && P.nx % 32 == 0 && !CHR) {
         const long long rows = (long long)P.ny * P.nz;
         const unsigned blocks = (unsigned)((rows + XW_WARPS - 1) / XW_WARPS);
         k_sweep_x_warp<R, FVS, RC><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
@@ -70,15 +71,22 @@ cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl
     const int seg = L.seg[DIR] > 0 ? L.seg[DIR] : segment_for(len, (long long)ext * other);
     const int th = threads_for(ext);
     dim3 grid((ext + th - 1) / th, other, (len + seg - 1) / seg);
-    k_sweep<DIR, R, FVS, RC><<<grid, th, 0, L.stream>>>(P, W, tacc, seg, ctrl);
+    k_sweep<DIR, R, FVS, RC, CHR><<<grid, th, 0, L.stream>>>(P, W, tacc, seg, ctrl);
     return cudaGetLastError();
 }
 
+// Characteristic-wise sweeps (L.chr) march every direction per thread (the
+// x warp kernel is component-wise only).
 template <class R, int FVS, int RC>
 cudaError_t sweeps(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl) {
-    if (dir == 0) return sweep_dir<0, R, FVS, RC>(L, W, tacc, ctrl);
-    if (dir == 1) return sweep_dir<1, R, FVS, RC>(L, W, tacc, ctrl);
-    return sweep_dir<2, R, FVS, RC>(L, W, tacc, ctrl);
+    if (L.chr) {
+        if (dir == 0) return sweep_dir<0, R, FVS, RC, true>(L, W, tacc, ctrl);
+        if (dir == 1) return sweep_dir<1, R, FVS, RC, true>(L, W, tacc, ctrl);
+        return sweep_dir<2, R, FVS, RC, true>(L, W, tacc, ctrl);
+    }
+    if (dir == 0) return sweep_dir<0, R, FVS, RC, false>(L, W, tacc, ctrl);
+    if (dir == 1) return sweep_dir<1, R, FVS, RC, false>(L, W, tacc, ctrl);
+    return sweep_dir<2, R, FVS, RC, false>(L, W, tacc, ctrl);
 }
 
 template <class R, int FVS>

@@ -17,6 +17,8 @@ Workloads (periodic [0, 2 pi)^3, gamma 1.4, Pr 0.72, CFL 0.5, C8th viscous):
            and FP32-stencil forms, errors of the latter against the former
   iso512   isotropic 512^3, Mach_t 0.4, Re 2000, k0 4, FP32-stencil form,
            UPWIND_7TH and WENO5, 100 steps, per-kernel HBM roofline
+  iso128char  the iso128 field with characteristic-wise reconstruction
+           (char_recon), SW + WENO5, FP64 and FP32-stencil forms, 200 steps
 (the adjoint workload, Taylor-Green 64^3, runs through bench.py / the tests).
 The isotropic Ma is solver.in's 0.5; Sutherland S/Tref is 110.4/273.15 for the
 Taylor-Green workloads, the reference's 110.4/288.15 otherwise.
@@ -43,6 +45,9 @@ WORKLOADS = {
                    recons=("mdcd",), steps=200, monitor=50, precisions=("fp64",)),
     "iso256": dict(kind="iso", n=256, Ma=0.5, mach_t=0.5, Re=1000.0, fvs="stagerwarming",
                    recons=("weno5",), steps=500, monitor=100, precisions=("fp64", "fp32acc64")),
+    "iso128char": dict(kind="iso", n=128, Ma=0.5, mach_t=0.3, Re=500.0, fvs="stagerwarming",
+                       recons=("weno5",), steps=200, monitor=50, precisions=("fp64", "fp32acc64"),
+                       char_recon=True),
     "iso512": dict(kind="iso", n=512, Ma=0.5, mach_t=0.4, Re=2000.0, fvs="stagerwarming",
                    recons=("upwind_7th", "weno5"), steps=100, monitor=50,
                    precisions=("fp32acc64",)),
@@ -63,6 +68,8 @@ def params_for(w: dict, recon: str, precision: str, dt_fixed: float = -1.0) -> S
               precision=precision)
     if "sutherland" in w:
         kw["sutherland_s_over_tref"] = w["sutherland"]
+    if w.get("char_recon"):
+        kw["char_recon"] = 1
     p = SolverParams.default().replace(**kw)
     if recon == "ud7l":
         p.ud7l_alpha = 1.0
@@ -140,13 +147,14 @@ def run(name: str, device: int = 0, steps: int | None = None) -> dict:
     for recon in w["recons"]:
         for prec in w["precisions"]:
             res["runs"].append(run_one(w, W, recon, prec, n_steps, device))
-    if name == "iso256":
+    if "fp64" in w["precisions"] and "fp32acc64" in w["precisions"]:
         # FP32-stencil vs FP64 at one fixed dt: end-time KE, dissipation, E(k)
-        with Solver(params_for(w, "weno5", "fp64"), device=device) as s:
+        rc = w["recons"][0]
+        with Solver(params_for(w, rc, "fp64"), device=device) as s:
             s.upload_primitive(W)
             dt0 = s.compute_timestep()
-        a = run_one(w, W, "weno5", "fp64", n_steps, device, dt_fixed=dt0)
-        b = run_one(w, W, "weno5", "fp32acc64", n_steps, device, dt_fixed=dt0)
+        a = run_one(w, W, rc, "fp64", n_steps, device, dt_fixed=dt0)
+        b = run_one(w, W, rc, "fp32acc64", n_steps, device, dt_fixed=dt0)
         ma, mb = a["monitors"][-1], b["monitors"][-1]
         Ea, Eb = np.array(a["final_spectrum"]), np.array(b["final_spectrum"])
         big = Ea > 1e-6 * Ea.max()

@@ -11,7 +11,7 @@ import pytest
 
 import ns3d_cpp_b200 as ns
 from ns3d_cpp_b200 import initial
-from conftest import SCHEMES, ref_cfg, relerr, scheme_id
+from conftest import CHAR_SCHEMES, SCHEMES, ref_cfg, relerr, scheme_id
 
 pytestmark = pytest.mark.gpu
 
@@ -190,6 +190,64 @@ def test_fp32_stencils_close_to_fp64(oracle_mod, kw):
         s.step(10)
         Wg = s.download_primitive()
     assert np.all(relerr(rhs, o.rhs(W)) <= 5e-5)
+    Wo = W
+    for _ in range(10):
+        Wo, _, st = o.cfl_step(Wo)
+    assert np.all(relerr(Wg, Wo) <= 1e-5)
+
+
+@pytest.mark.parametrize("kw", CHAR_SCHEMES, ids=scheme_id)
+def test_char_recon_rhs_fp64_matches_oracle(oracle_mod, kw):
+    """Characteristic-wise reconstruction (du_inviscous_character): RHS on a
+    cube and on a box whose x extent is a multiple of 32 (the x lines march
+    per thread on this path)."""
+    for shape in [(16, 16, 16), (12, 16, 32)]:
+        nz, ny, nx = shape
+        cfg = ref_cfg(nx, **kw)
+        cfg.update(global_ny=ny, global_nz=nz, Ly=2 * np.pi * ny / nx, Lz=2 * np.pi * nz / nx)
+        W = initial.taylor_green(nx, Ma=0.1, perturb=0.05, seed=11)[:, :nz, :ny, :]
+        W = np.ascontiguousarray(W)
+        with ns.Solver(params_from_cfg(cfg)) as s:
+            s.upload_primitive(W)
+            rhs = s.compute_rhs()
+        ref = oracle_mod.Oracle(cfg).rhs(W)
+        err = relerr(rhs, ref)
+        assert np.all(err <= TOL64), (shape, err)
+
+
+@pytest.mark.parametrize("kw", CHAR_SCHEMES, ids=scheme_id)
+def test_char_recon_cfl_steps_fp64_match_oracle(oracle_mod, kw):
+    n = 12
+    cfg = ref_cfg(n, **kw)
+    W = tgv_input(n, seed=3)
+    o = oracle_mod.Oracle(cfg)
+    Wo = W
+    for _ in range(5):
+        Wo, dt, st = o.cfl_step(Wo)
+        assert st == 0
+    with ns.Solver(params_from_cfg(cfg)) as s:
+        s.upload_primitive(W)
+        s.step(5)
+        assert abs(s.last_dt() - dt) <= 1e-14 * dt
+        Wg = s.download_primitive()
+    assert np.all(relerr(Wg, Wo) <= TOL64)
+
+
+@pytest.mark.parametrize("kw", CHAR_SCHEMES[:2], ids=scheme_id)
+def test_char_recon_fp32_close_to_fp64(oracle_mod, kw):
+    """FP32-stencil form of the characteristic path against the FP64 oracle,
+    with the tolerances of the component-wise FP32 test (RHS 5e-5, state
+    after 10 steps 1e-5)."""
+    n = 16
+    cfg = ref_cfg(n, **kw)
+    W = tgv_input(n, seed=9)
+    o = oracle_mod.Oracle(cfg)
+    with ns.Solver(params_from_cfg(cfg, precision="fp32acc64")) as s:
+        s.upload_primitive(W)
+        rhs = s.compute_rhs()
+        s.step(10)
+        Wg = s.download_primitive()
+    assert np.all(relerr(rhs, o.rhs(W)) <= 5e-5), relerr(rhs, o.rhs(W))
     Wo = W
     for _ in range(10):
         Wo, _, st = o.cfl_step(Wo)

@@ -145,7 +145,7 @@ def test_create_rejects_out_of_scope_configs():
     """Configurations the product does not build are refused before any GPU use."""
     base = SolverParams.default().replace(n=16)
     lib = _lib.load()
-    for kw in (dict(char_recon=1), dict(recon=1)):
+    for kw in (dict(recon=1),):
         p = base.replace(**kw)
         ctx = ctypes.c_void_p()
         assert lib.ns3d_create(ctypes.byref(p), 0, ctypes.byref(ctx)) == 2
