@@ -54,6 +54,55 @@ __device__ __forceinline__ int wrap1(int s, int len) {
 }
 
 // ---------------------------------------------------------------------------
+// One face of du_inviscous_character (InviscousFlux_new.cpp:165-437): the Roe
+// state of the face's two cells wl, wr (primitives, rho as stored), the
+// eigenvector matrices along DIR, the windows projected on the left
+// eigenvectors (sums from 0 in the reference's order), one reconstruction per
+// characteristic field and the result mapped back by the right ones.
+// FP(m, r) / FM(m, r): split flux component r of window cell m (unreversed;
+// the minus window is reversed here as reconstruct_select does). In the FP32
+// form the windows are deviations from a common offset, which the projection
+// and reconstruction carry through (R L ref = ref cancels in the difference).
+// ---------------------------------------------------------------------------
+template <int DIR, class R, int RC, class GP, class GM>
+__device__ __forceinline__ void char_face(double gamma, const double* wl, const double* wr,
+                                          GP FP, GM FM, const R* lin, R disp, R diss,
+                                          R face[5]) {
+    constexpr int S = Stencil<RC>::S;
+    double ua[5], Lm[5][5], Rm[5][5];
+    roe_state(gamma, wl, wr, ua);
+    eigen_LR<DIR == 0, DIR == 1, DIR == 2>(gamma, ua, Lm, Rm);
+    R wc[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        R a[S], bc[S], b[S];
+#pragma unroll
+        for (int m = 0; m < S; ++m) {
+            R sp = R(0.0), sm = R(0.0);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+                sp += R(Lm[q][r]) * FP(m, r);
+                sm += R(Lm[q][r]) * FM(m, r);
+            }
+            a[m] = sp;
+            bc[m] = sm;
+        }
+#pragma unroll
+        for (int m = 0; m < S; ++m) b[m] = bc[S - 1 - m];
+        const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+        const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+        wc[q] = plus_face + minus_face;
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        R sum = R(0.0);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) sum += R(Rm[q][r]) * wc[r];
+        face[q] = sum;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Inviscid sweep along DIR (du_inviscous, InviscousFlux_new.cpp:4-163, and the
 // divergence of range_kutta.cpp:51-98).
 //
@@ -158,47 +207,15 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     };
     (void)gamma;
     (void)eps;
-    // CHR: du_inviscous_character. The face's two cells are reloaded (L1/L2
-    // hits); rho unclamped, as the reference reads F.rho. In the FP32 form the
-    // windows are deviations from the segment's offset, which the projection
-    // and reconstruction carry through unchanged (R L ref = ref cancels in the
-    // face difference).
-    auto char_face = [&](int f, R* face) {
-        double wl[5], wr[5], ua[5], Lm[5][5], Rm[5][5];
+    // CHR: the face's two cells are reloaded (L1/L2 hits); rho as stored.
+    auto char_face_at = [&](int f, R* face) {
+        double wl[5], wr[5];
         load_raw(f, wl);
         load_raw(f + 1, wr);
-        roe_state(P.gamma, wl, wr, ua);
-        eigen_LR<DIR == 0, DIR == 1, DIR == 2>(P.gamma, ua, Lm, Rm);
-        R wc[5];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            R a[S], bc[S], b[S];
-#pragma unroll
-            for (int m = 0; m < S; ++m) {
-                R sp = R(0.0), sm = R(0.0);
-#pragma unroll
-                for (int r = 0; r < 5; ++r) {
-                    sp += R(Lm[q][r]) * fp[m][r];
-                    sm += R(Lm[q][r]) * fm[m][r];
-                }
-                a[m] = sp;
-                bc[m] = sm;
-            }
-#pragma unroll
-            for (int m = 0; m < S; ++m) b[m] = bc[S - 1 - m];
-            const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
-            const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
-            wc[q] = plus_face + minus_face;
-        }
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            R sum = R(0.0);
-#pragma unroll
-            for (int r = 0; r < 5; ++r) sum += R(Rm[q][r]) * wc[r];
-            face[q] = sum;
-        }
+        char_face<DIR, R, RC>(P.gamma, wl, wr, [&](int m, int r) { return fp[m][r]; },
+                              [&](int m, int r) { return fm[m][r]; }, lin, disp, diss, face);
     };
-    (void)char_face;
+    (void)char_face_at;
 
     int f = c0 - 1;  // face f sits between cells f and f+1 (the reference's i_face = f + ng)
     double nxt[5];
@@ -226,7 +243,7 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
         split_raw(cur, fp[S - 1], fm[S - 1], false);
         R face[5];
         if constexpr (CHR) {
-            char_face(f, face);
+            char_face_at(f, face);
         } else if constexpr (kDeviation && RC == RC_WENO5) {
             // reconstruct_select reverses the minus window (flag < 0)
             weno5_face_x2([&](int m, int q) { return fp[m][q]; },
@@ -280,7 +297,7 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
 // ---------------------------------------------------------------------------
 constexpr int XW_WARPS = 4;
 
-template <class R, int FVS, int RC>
+template <class R, int FVS, int RC, bool CHR = false>
 __global__ void __launch_bounds__(32 * XW_WARPS)
 k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
@@ -356,8 +373,25 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
         }
     };
     // face at chunk-relative position `pos` (face pos sits between cells pos and
-    // pos+1 of the chunk in slot `cs`); window cells pos-MID .. pos-MID+S-1
-    auto face_at = [&](int cs, int pos, R* face) {
+    // pos+1 of chunk `chunk`, held in slot `cs`); window cells pos-MID .. pos-MID+S-1
+    auto face_at = [&](int cs, int pos, int chunk, R* face) {
+        if constexpr (CHR) {
+            // the face's two cells, loaded coalesced over the warp (rho as stored)
+            auto at = [&](int m) {
+                int k = cs * 32 + pos - MID + m;
+                return k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
+            };
+            int gl = chunk * 32 + pos;
+            gl = gl < 0 ? gl + nx : gl;
+            const int gr = gl + 1 == nx ? 0 : gl + 1;
+            const double wl[5] = {W.rho[base + gl], W.u[base + gl], W.v[base + gl],
+                                  W.w[base + gl], W.p[base + gl]};
+            const double wr[5] = {W.rho[base + gr], W.u[base + gr], W.v[base + gr],
+                                  W.w[base + gr], W.p[base + gr]};
+            char_face<0, R, RC>(P.gamma, wl, wr, [&](int m, int r) { return rp[r][at(m)]; },
+                                [&](int m, int r) { return rm[r][at(m)]; }, lin, disp, diss, face);
+            return;
+        }
         if constexpr (kDeviation && RC == RC_WENO5) {
             auto at = [&](int m) {
                 int k = cs * 32 + pos - MID + m;
@@ -401,7 +435,7 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     __syncwarp();
     // the face on the -x side of cell 0 (face nx-1 by periodicity)
     R carry[5];
-    face_at(1, -1, carry);
+    face_at(1, -1, 0, carry);
     int cur = 1;
     for (int c = 0; c < nch; ++c) {
         const int nslot = cur == 2 ? 0 : cur + 1;
@@ -421,7 +455,7 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
         const long long id = base + (c << 5) + lane;
         __syncwarp();
         R face[5];
-        face_at(cur, lane, face);
+        face_at(cur, lane, c, face);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             R left = __shfl_up_sync(0xffffffffu, face[q], 1);

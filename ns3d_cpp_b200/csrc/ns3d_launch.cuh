@@ -59,10 +59,10 @@ namespace detail {
 template <int DIR, class R, int FVS, int RC, bool CHR>
 cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl) {
     const DevParams& P = L.P;
-    if (DIR == 0 && P.nx % 32 == 0 && !CHR) {
+    if (DIR == 0 && P.nx % 32 == 0) {
         const long long rows = (long long)P.ny * P.nz;
         const unsigned blocks = (unsigned)((rows + XW_WARPS - 1) / XW_WARPS);
-        k_sweep_x_warp<R, FVS, RC><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
+        k_sweep_x_warp<R, FVS, RC, CHR><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
         return cudaGetLastError();
     }
     const int ext = DIR == 0 ? P.ny : P.nx;        // thread dimension
@@ -75,8 +75,7 @@ cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl
     return cudaGetLastError();
 }
 
-// Characteristic-wise sweeps (L.chr) march every direction per thread (the
-// x warp kernel is component-wise only).
+// L.chr selects the characteristic-wise sweeps (du_inviscous_character).
 template <class R, int FVS, int RC>
 cudaError_t sweeps(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl) {
     if (L.chr) {

@@ -199,9 +199,9 @@ def test_fp32_stencils_close_to_fp64(oracle_mod, kw):
 @pytest.mark.parametrize("kw", CHAR_SCHEMES, ids=scheme_id)
 def test_char_recon_rhs_fp64_matches_oracle(oracle_mod, kw):
     """Characteristic-wise reconstruction (du_inviscous_character): RHS on a
-    cube and on a box whose x extent is a multiple of 32 (the x lines march
-    per thread on this path)."""
-    for shape in [(16, 16, 16), (12, 16, 32)]:
+    cube (x lines marched per thread) and on boxes whose x extent is a
+    multiple of 32 (the warp-per-row x sweep, 1 and 3 chunks per row)."""
+    for shape in [(16, 16, 16), (12, 16, 32), (8, 8, 96)]:
         nz, ny, nx = shape
         cfg = ref_cfg(nx, **kw)
         cfg.update(global_ny=ny, global_nz=nz, Ly=2 * np.pi * ny / nx, Lz=2 * np.pi * nz / nx)
