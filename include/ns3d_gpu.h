@@ -93,11 +93,17 @@ typedef struct ns3d_turb_stats {
     double kinetic_energy;  /* <0.5|u|^2> */
     double tke;             /* 0.5 (var u + var v + var w) */
     double u_rms;           /* sqrt(<|u|^2>/3) */
-    double dissipation;     /* 2 nu sum_k k^2 E(k), nu = <mu(T)>/<rho> */
+    double dissipation;     /* eps = 2 nu sum_k k^2 E(k), nu = <mu(T)>/<rho> */
     double nu, mean_mu, mean_rho;
     double mach_t;          /* sqrt(2 KE) / <c> */
     double total_energy;    /* sum 0.5 rho |u|^2 dV (compute_total_energy, postprocess.cpp:103) */
-    double reserved[7];
+    double taylor;          /* Taylor microscale sqrt(15 nu u_rms^2 / eps) */
+    double eta;             /* Kolmogorov length (nu^3 / eps)^(1/4) */
+    double u_eta;           /* Kolmogorov velocity (nu eps)^(1/4) */
+    double tau_eta;         /* Kolmogorov time (nu / eps)^(1/2) */
+    double taylor_li;       /* u_rms / sqrt(<(du/dx)^2>) */
+    double re_lambda;       /* u_rms taylor_li / nu */
+    double dudx2;           /* <(du/dx)^2>, du/dx of compute_gradients_dudx (ViscousFlux.cpp:389) */
 } ns3d_turb_stats;
 
 /* ---- parameters ---------------------------------------------------------- */
@@ -253,7 +259,20 @@ ns3d_status ns3d_total_energy(ns3d_ctx *ctx, double *etot);
 /* compute_energy_spectrum (EnergySpectrum.cpp:62-125): E(k), k = 0..nbins-1,
  * nbins <= 2*global_nx + 1; transform of u,v,w scaled by 1/N, shells by floor(|k|). */
 ns3d_status ns3d_energy_spectrum(ns3d_ctx *ctx, double *Ek, int nbins);
-/* compute_turbulence_statistics, KE and dissipation parts (ana_isotropic.cpp:241-303). */
+/* init_isotropic_turbulence (isotropic_ini.cpp:146-193) with generate_full_turbulence
+ * (:25-122) into the context's state: a random-phase solenoidal velocity with spectrum
+ * ~ kk exp(-2 kk / k0^2), the phases drawn from mt19937_64(seed) + uniform [0, 1) in the
+ * reference's order (no draws for k = 0), inverse transforms on the device (cuFFT),
+ * rho = 1, T = 1, p = Rgas. mach_t <= 0 normalises the mean 0.5|u|^2 to
+ * Ek0 = 3A/64 sqrt(2 pi) k0^5 as the reference does; mach_t > 0 scales the velocity
+ * to that turbulent Mach number sqrt(2 KE) / <c> instead. k0 = 8, A = 0.00013,
+ * seed = 123, mach_t = 0 reproduce the reference's first call in a process (its
+ * generator keeps one static stream per process). Allocates and frees its scratch
+ * (72 bytes per cell on the device). */
+ns3d_status ns3d_init_isotropic(ns3d_ctx *ctx, int k0, double A, unsigned long long seed,
+                                double mach_t);
+/* compute_turbulence_statistics (ana_isotropic.cpp:196-314): every quantity of its
+ * statistics row, without the rank-0 gather and the spectrum file round trip. */
 ns3d_status ns3d_turbulence_stats(ns3d_ctx *ctx, ns3d_turb_stats *out);
 
 #ifdef __cplusplus

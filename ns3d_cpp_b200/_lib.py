@@ -51,6 +51,7 @@ _SIGS = {
     "ns3d_total_energy": (_i, [_vp, _D]),
     "ns3d_energy_spectrum": (_i, [_vp, _D, _i]),
     "ns3d_turbulence_stats": (_i, [_vp, _vp]),
+    "ns3d_init_isotropic": (_i, [_vp, _i, ctypes.c_double, ctypes.c_ulonglong, ctypes.c_double]),
     "ns3d_get_stream": (_i, [_vp, _pvp]),
     "ns3d_profile": (_i, [_vp, _i]),
     "ns3d_profile_read": (_i, [_vp, _D, ctypes.POINTER(ctypes.c_longlong)]),

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -184,6 +185,66 @@ __global__ void k_prim_finish(DevParams P, StateOut W) {
     double rr = W.rho[id];
     if (rr <= 0.0) { rr = 1e-12; W.rho[id] = rr; }
     W.T[id] = W.p[id] / (rr * P.Rgas);
+}
+
+// ---- isotropic initial field (generate_full_turbulence, isotropic_ini.cpp:25-122)
+
+// Fourier coefficients of the three velocity components at every mode:
+// amplitude sqrt(2/3) sqrt(A kk exp(-2 kk / k0^2) / 4 pi), three random phases
+// 2 pi r, projection normal to k. r: the uniform draws of the reference's
+// loop order (z outermost, x innermost = this layout's order), 3 per cell,
+// none for k = 0. Same expressions and operation order as the reference.
+__global__ void k_iso_modes(int NX, int NY, int NZ, int k0, double A, const double* __restrict__ r,
+                            cufftDoubleComplex* __restrict__ U, cufftDoubleComplex* __restrict__ V,
+                            cufftDoubleComplex* __restrict__ Wc) {
+    const long long n = (long long)NX * NY * NZ;
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const double PI = 3.14159265358979323846;
+    const int i = (int)(id % NX), j = (int)((id / NX) % NY), k = (int)(id / ((long long)NX * NY));
+    const int k1 = (i <= NX / 2 ? i : i - NX);
+    const int k2 = (j <= NY / 2 ? j : j - NY);
+    const int k3 = (k <= NZ / 2 ? k : k - NZ);
+    const int kk = k1 * k1 + k2 * k2 + k3 * k3;
+    if (kk == 0) {
+        U[id] = make_cuDoubleComplex(0.0, 0.0);
+        V[id] = make_cuDoubleComplex(0.0, 0.0);
+        Wc[id] = make_cuDoubleComplex(0.0, 0.0);
+        return;
+    }
+    const double Ak = sqrt(2.0 / 3.0) * sqrt(A * kk * exp(-2.0 * kk / (double)(k0 * k0)) / (4.0 * PI));
+    const double a1 = 2 * PI * r[3 * id], a2 = 2 * PI * r[3 * id + 1], a3 = 2 * PI * r[3 * id + 2];
+    const double v1r = Ak * sin(a1), v1i = Ak * cos(a1);
+    const double v2r = Ak * sin(a2), v2i = Ak * cos(a2);
+    const double v3r = Ak * sin(a3), v3i = Ak * cos(a3);
+    const double vkr = k1 * v1r + k2 * v2r + k3 * v3r;
+    const double vki = k1 * v1i + k2 * v2i + k3 * v3i;
+    U[id] = make_cuDoubleComplex(k1 * vkr / kk - v1r, k1 * vki / kk - v1i);
+    V[id] = make_cuDoubleComplex(k2 * vkr / kk - v2r, k2 * vki / kk - v2i);
+    Wc[id] = make_cuDoubleComplex(k3 * vkr / kk - v3r, k3 * vki / kk - v3i);
+}
+
+// Real parts of the inverse transforms as the velocity, rho = 1, T = 1,
+// p = Rgas rho T (init_isotropic_turbulence, isotropic_ini.cpp:184-189).
+__global__ void k_iso_state(DevParams P, const cufftDoubleComplex* __restrict__ U,
+                            const cufftDoubleComplex* __restrict__ V,
+                            const cufftDoubleComplex* __restrict__ Wc, StateOut W) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= P.n) return;
+    W.rho[id] = 1.0;
+    W.u[id] = U[id].x;
+    W.v[id] = V[id].x;
+    W.w[id] = Wc[id].x;
+    W.p[id] = P.Rgas * 1.0 * 1.0;
+    W.T[id] = 1.0;
+}
+
+__global__ void k_iso_scale(long long n, double s, StateOut W) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    W.u[id] *= s;
+    W.v[id] *= s;
+    W.w[id] *= s;
 }
 
 // conservedToPrimitive (+ T) of an uploaded conserved state held in `U`.
@@ -1087,6 +1148,90 @@ ns3d_status ns3d_turbulence_stats(ns3d_ctx* ctx, ns3d_turb_stats* out) {
     double eps = 0.0;
     for (int k = 0; k < kmax; ++k) eps += 2.0 * out->nu * (double)k * (double)k * Ek[k];
     out->dissipation = eps;
+    // ana_isotropic.cpp:286-303
+    out->dudx2 = s[12] / N;
+    out->taylor_li = out->u_rms / std::sqrt(out->dudx2);
+    out->re_lambda = out->u_rms * out->taylor_li / out->nu;
+    out->eta = std::pow(out->nu * out->nu * out->nu / eps, 0.25);
+    out->u_eta = std::pow(out->nu * eps, 0.25);
+    out->tau_eta = std::pow(out->nu / eps, 0.5);
+    out->taylor = std::sqrt(15.0 * out->nu * out->u_rms * out->u_rms / eps);
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_init_isotropic(ns3d_ctx* ctx, int k0, double A, unsigned long long seed,
+                                double mach_t) {
+    if (!ctx || k0 <= 0 || !(A > 0.0)) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const int NX = ctx->p.global_nx, NY = ctx->p.global_ny, NZ = ctx->p.global_nz;
+    const long long n = ctx->n;
+    const size_t plane = (size_t)3 * NX * NY;
+    DevBuf r, spec;
+    double* host = nullptr;
+    if (!r.alloc((size_t)3 * n) || !spec.alloc((size_t)6 * n) ||
+        cudaMallocHost(&host, sizeof(double) * plane) != cudaSuccess)
+        return fail(ctx, NS3D_ERR_NOMEM, "init_isotropic: scratch allocation failed");
+    // the uniform draws, in the reference's order (rnd01: mt19937_64 + uniform [0,1))
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    ns3d_status st = NS3D_OK;
+    for (int k = 0; k < NZ && st == NS3D_OK; ++k) {
+        size_t q = 0;
+        for (int j = 0; j < NY; ++j)
+            for (int i = 0; i < NX; ++i) {
+                if (i == 0 && j == 0 && k == 0) {  // kk == 0: no draws
+                    host[q++] = 0.0; host[q++] = 0.0; host[q++] = 0.0;
+                    continue;
+                }
+                host[q++] = dist(rng);
+                host[q++] = dist(rng);
+                host[q++] = dist(rng);
+            }
+        if (cudaMemcpyAsync(r.p + (size_t)k * plane, host, sizeof(double) * plane,
+                            cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            st = fail(ctx, NS3D_ERR_CUDA, "init_isotropic: copy of the phases failed");
+    }
+    cudaFreeHost(host);
+    if (st != NS3D_OK) return st;
+    auto* U = reinterpret_cast<cufftDoubleComplex*>(spec.p);
+    auto* V = U + n;
+    auto* Wc = V + n;
+    k_iso_modes<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(NX, NY, NZ, k0, A, r.p, U, V, Wc);
+    NS3D_CK(cudaGetLastError());
+    // inverse (backward, unnormalised) transforms, as fftw_plan_dft_3d(..., FFTW_BACKWARD)
+    cufftHandle plan;
+    if (cufftPlan3d(&plan, NZ, NY, NX, CUFFT_Z2Z) != CUFFT_SUCCESS)
+        return fail(ctx, NS3D_ERR_CUDA, "init_isotropic: cufftPlan3d failed");
+    cufftSetStream(plan, ctx->stream);
+    bool ok = true;
+    for (cufftDoubleComplex* c : {U, V, Wc}) ok = ok && cufftExecZ2Z(plan, c, c, CUFFT_INVERSE) == CUFFT_SUCCESS;
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    cufftDestroy(plan);
+    if (!ok) return fail(ctx, NS3D_ERR_CUDA, "init_isotropic: cufftExecZ2Z failed");
+    k_iso_state<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(ctx->L.P, U, V, Wc, outv(ctx, ctx->cur));
+    NS3D_CK(cudaGetLastError());
+    // energy normalisation: mean 0.5|u|^2 -> Ek0 = 3A/64 sqrt(2 pi) k0^5 (isotropic_ini.cpp:36,
+    // 106-118), or the turbulent Mach number sqrt(2 KE) / <c> -> mach_t
+    double sums[NSUMS];
+    if ((st = compute_sums(ctx, sums)) != NS3D_OK) return st;
+    const double PI = 3.14159265358979323846;
+    const double Er = sums[1] / (double)n;
+    double scale;
+    if (mach_t > 0.0) {
+        const double c_mean = sums[11] / (double)n;
+        scale = mach_t * c_mean / std::sqrt(2.0 * Er);
+    } else {
+        const double Ek0 = 3.0 * A / 64.0 * std::sqrt(2 * PI) * std::pow(k0, 5);
+        scale = std::sqrt(Ek0 / Er);
+    }
+    k_iso_scale<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(n, scale, outv(ctx, ctx->cur));
+    NS3D_CK(cudaGetLastError());
+    k_prim_finish<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(ctx->L.P, outv(ctx, ctx->cur));
+    NS3D_CK(cudaGetLastError());
+    ctx->rec = ctx->cur;
+    ctx->dtmin_valid = false;
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
     return NS3D_OK;
 }
 

@@ -908,7 +908,7 @@ k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
 }
 
 // Sums of the reductions below (see k_sums_partial).
-constexpr int NSUMS = 12;
+constexpr int NSUMS = 13;
 
 // The kernels from here on are not templates; only the API translation unit
 // (which defines NS3D_API_KERNELS) instantiates them.
@@ -985,7 +985,16 @@ __global__ void k_control_post(Ctrl* c, int mode, double total_time, long long n
 // compute_turbulence_statistics (ana_isotropic.cpp:241-255), per block, then
 // a second pass sums the block partials in double. Outputs 12 sums:
 // [0] sum 0.5 rho |u|^2, [1] sum 0.5|u|^2, [2] sum mu(T), [3] sum rho,
-// [4] sum |u|^2, [5..7] sum u,v,w, [8..10] sum u^2,v^2,w^2, [11] sum sqrt(g R T).
+// [4] sum |u|^2, [5..7] sum u,v,w, [8..10] sum u^2,v^2,w^2, [11] sum sqrt(g R T),
+// [12] sum (du/dx)^2 with du/dx of compute_gradients_dudx (ViscousFlux.cpp:389-410):
+// the viscous scheme's central derivative.
+template <int ORD>
+__device__ __forceinline__ double dudx_at(const DevParams& P, const double* __restrict__ u,
+                                          long long id) {
+    const int nx = P.nx;
+    const int i = (int)(id % nx);
+    return dcentral<double, ORD>([&](int o) { return u[id + (wrap1(i + o, nx) - i)]; }, P.dx);
+}
 
 __global__ void __launch_bounds__(256)
 k_sums_partial(DevParams P, StateView W, double* __restrict__ part) {
@@ -1008,6 +1017,9 @@ k_sums_partial(DevParams P, StateView W, double* __restrict__ part) {
         s[9] += v * v;
         s[10] += w * w;
         s[11] += sqrt(P.gamma * P.Rgas * T);
+        const double dudx = P.vis_order == 4 ? dudx_at<4>(P, W.u, id)
+                          : (P.vis_order == 6 ? dudx_at<6>(P, W.u, id) : dudx_at<8>(P, W.u, id));
+        s[12] += dudx * dudx;
     }
     __shared__ double red[NSUMS][8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

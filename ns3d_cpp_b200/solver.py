@@ -104,7 +104,8 @@ class SolverParams(ctypes.Structure):
 class TurbStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ("kinetic_energy", "tke", "u_rms", "dissipation", "nu", "mean_mu", "mean_rho",
-                 "mach_t", "total_energy")] + [("reserved", ctypes.c_double * 7)]
+                 "mach_t", "total_energy", "taylor", "eta", "u_eta", "tau_eta", "taylor_li",
+                 "re_lambda", "dudx2")]
 
 
 def _check(status: int, ctx=None) -> None:
@@ -315,4 +316,12 @@ class Solver:
     def compute_turbulence_statistics(self) -> dict:
         s = TurbStats()
         self._ck(self.lib.ns3d_turbulence_stats(self.ctx, ctypes.byref(s)))
-        return {n: getattr(s, n) for n, _ in TurbStats._fields_ if n != "reserved"}
+        return {n: getattr(s, n) for n, _ in TurbStats._fields_}
+
+    def init_isotropic(self, k0: int = 8, A: float = 0.00013, seed: int = 123,
+                       mach_t: float = 0.0) -> None:
+        """init_isotropic_turbulence (isotropic_ini.cpp:146-193) on the device: the
+        defaults reproduce the reference's field; mach_t > 0 scales the velocity
+        to that turbulent Mach number instead of the reference's energy Ek0."""
+        self._ck(self.lib.ns3d_init_isotropic(self.ctx, int(k0), float(A), int(seed),
+                                              float(mach_t)))

@@ -673,8 +673,10 @@ double orc_total_energy(const orc_params *P, const double *W) {
  * out = [sum 0.5|u|^2, sum mu(T), sum rho, sum |u|^2, sum u, sum v, sum w,
  *        sum u^2, sum v^2, sum w^2, sum sqrt(gamma Rgas T)]. */
 void orc_turb_sums(const orc_params *P, const double *W, double *out) {
+    const int nx = P->nx, ny = P->ny;
     const long n = (long)P->nx * P->ny * P->nz;
-    double s[11] = {0};
+    const int ord = vis_order(P->vis);
+    double s[12] = {0};
     for (long t = 0; t < n; ++t) {
         double rho = W[t], uu = W[n + t], vv = W[2 * n + t], ww = W[3 * n + t], p = W[4 * n + t];
         double T = p / (rho * P->Rgas);
@@ -685,6 +687,10 @@ void orc_turb_sums(const orc_params *P, const double *W, double *out) {
         s[4] += uu; s[5] += vv; s[6] += ww;
         s[7] += uu * uu; s[8] += vv * vv; s[9] += ww * ww;
         s[10] += sqrt(P->gamma * P->Rgas * T);
+        /* du/dx of compute_gradients_dudx (ViscousFlux.cpp:389-410), the viscous order */
+        const double dudx = dcentral(W + n, t, 1, (int)(t % nx), nx, ord, P->dx);
+        s[11] += dudx * dudx;
     }
+    (void)ny;
     memcpy(out, s, sizeof(s));
 }

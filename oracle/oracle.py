@@ -209,7 +209,7 @@ class Oracle:
         return Fv, g
 
     def turb_sums(self, W):
-        out = np.zeros(11)
+        out = np.zeros(12)
         self.lib.orc_turb_sums(ctypes.byref(self.p), _dp(self._w(W)), _dp(out))
         return out
 
@@ -450,5 +450,12 @@ def turbulence_stats(sums: np.ndarray, Ek: np.ndarray, N: int, gamma: float, Rga
     eps = 0.0
     for i in range(len(Ek)):
         eps += 2.0 * nu * k[i] * k[i] * Ek[i]
+    # ana_isotropic.cpp:286-303: Taylor length from <(du/dx)^2>, Kolmogorov scales,
+    # Taylor microscale
+    dudx2 = s[11] / N
+    taylor_li = u_rms / math.sqrt(dudx2)
     return dict(kinetic_energy=ke, tke=tke, u_rms=u_rms, dissipation=eps, nu=nu, Mach_t=mach_t,
-                mean_mu=mean_mu, mean_rho=mean_rho)
+                mean_mu=mean_mu, mean_rho=mean_rho, dudx2=dudx2, taylor_Li=taylor_li,
+                Re_lambda=u_rms * taylor_li / nu, eta=math.pow(nu * nu * nu / eps, 0.25),
+                u_eta=math.pow(nu * eps, 0.25), tau_eta=math.pow(nu / eps, 0.5),
+                taylor=math.sqrt(15.0 * nu * u_rms * u_rms / eps))

@@ -6,7 +6,8 @@ Each fixture holds the outputs of the reference's own compute_rhs,
 compute_timestep + runge_kutta_3 (two CFL steps) and, for the isotropic case,
 isotropic_post_process (spectrum file, 6 significant digits, and the stats row,
 8 digits) for a deterministic input built by `golden_input` below, so the
-inputs need not be stored.
+inputs need not be stored; isotropic_ic.npz holds the reference's own
+init_isotropic_turbulence field (rho, u, v, w, p) for the boxes IC_BOXES.
 """
 import os
 import sys
@@ -83,8 +84,37 @@ def main():
     np.savez_compressed(os.path.join(HERE, "isotropic_post_16.npz"), k=k, Ek=Ek,
                         stats=np.array([stats[s] for s in sorted(stats)]),
                         stat_names=np.array(sorted(stats)), ke=r.total_energy())
+    # the reference's own initial field (init_isotropic_turbulence), one fresh
+    # process per box: its generator keeps a static random stream per process
+    import subprocess
+    ic = {}
+    for nx, ny, nz in IC_BOXES:
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "ic.npy")
+            subprocess.run([sys.executable, __file__, "--ic", str(nx), str(ny), str(nz), out],
+                           check=True, stdout=subprocess.DEVNULL)
+            ic[f"{nx}x{ny}x{nz}"] = np.load(out)
+    np.savez_compressed(os.path.join(HERE, "isotropic_ic.npz"), **ic)
     print("golden fixtures written")
 
 
+# boxes of the initial-field fixture (nx, ny, nz)
+IC_BOXES = [(16, 16, 16), (16, 12, 8)]
+
+
+def ic_cfg(nx, ny, nz):
+    return ref_cfg(nx, Ma=0.5, Re=500, global_ny=ny, global_nz=nz)
+
+
+def _ic_case(nx, ny, nz, out):
+    import oracle
+    r = oracle.Ref(ic_cfg(nx, ny, nz))
+    r.init_isotropic()
+    np.save(out, r.W())
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "--ic":
+        _ic_case(int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4]), sys.argv[5])
+    else:
+        main()

@@ -170,7 +170,36 @@ def test_reductions_match_oracle(oracle_mod):
     so = oracle_mod.turbulence_stats(o.turb_sums(W), Eo, n ** 3, o.d["gamma"], o.d["Rgas"])
     for k in ("kinetic_energy", "tke", "u_rms", "dissipation", "nu"):
         assert abs(st[k] - so[k]) <= 1e-11 * abs(so[k]), k
+    # the rest of the statistics row (ana_isotropic.cpp:286-303)
+    for k, ko in (("dudx2", "dudx2"), ("taylor_li", "taylor_Li"), ("re_lambda", "Re_lambda"),
+                  ("eta", "eta"), ("u_eta", "u_eta"), ("tau_eta", "tau_eta"),
+                  ("taylor", "taylor")):
+        assert abs(st[k] - so[ko]) <= 1e-11 * abs(so[ko]), k
     assert abs(st["mach_t"] - 0.3) < 1e-12
+
+
+def test_init_isotropic_matches_reference_golden():
+    """init_isotropic_turbulence on the device (cuFFT) against the reference's
+    own field (tests/golden/isotropic_ic.npz, generated by its FFTW-API build
+    from the same mt19937_64 phases): rho and p bit-equal, velocity 1e-12.
+    mach_t > 0 scales the same field to that turbulent Mach number."""
+    from golden.make_golden import IC_BOXES, ic_cfg
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "isotropic_ic.npz"))
+    for nx, ny, nz in IC_BOXES:
+        ref = g[f"{nx}x{ny}x{nz}"]
+        with ns.Solver(params_from_cfg(ic_cfg(nx, ny, nz))) as s:
+            s.init_isotropic()
+            W = s.download_primitive()
+            s.init_isotropic(mach_t=0.3)
+            Wm = s.download_primitive()
+            st = s.compute_turbulence_statistics()
+        assert np.array_equal(W[0], ref[0]) and np.array_equal(W[4], ref[4])
+        err = relerr(W[1:4], ref[1:4])
+        assert np.all(err <= 1e-12), (nx, ny, nz, err)
+        assert abs(st["mach_t"] - 0.3) <= 1e-12
+        ratio = Wm[1:4].ravel() / W[1:4].ravel()
+        big = np.abs(W[1:4].ravel()) > 1e-3 * np.abs(W[1:4]).max()
+        assert np.ptp(ratio[big]) <= 1e-12 * abs(ratio[big][0])
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(fvs_type="LaxFriedrichs", recon="MDCD"),

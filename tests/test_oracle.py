@@ -263,8 +263,12 @@ def test_spectrum_and_stats_match_reference_golden(oracle_mod):
     Ek6 = np.array([float(f"{e:.6g}") for e in Ek])
     s6 = oracle_mod.turbulence_stats(o.turb_sums(W), Ek6, 16 ** 3, d["gamma"], d["Rgas"])
     s = oracle_mod.turbulence_stats(o.turb_sums(W), Ek, 16 ** 3, d["gamma"], d["Rgas"])
-    for name in ("kinetic_energy", "tke", "u_rms", "Mach_t"):
+    for name in ("kinetic_energy", "tke", "u_rms", "Mach_t", "taylor_Li"):
         assert abs(s[name] - stats[name]) <= 1e-7 * abs(stats[name]), name
     assert abs(s6["dissipation"] - stats["dissipation"]) <= 1e-7 * stats["dissipation"]
+    # Re_lambda needs no spectrum; the Kolmogorov and Taylor scales use the
+    # dissipation of the 6-digit spectrum (the stats row holds 8 digits)
+    for name in ("Re_lambda", "eta", "u_eta", "tau_eta", "taylor"):
+        assert abs(s6[name] - stats[name]) <= 1e-7 * abs(stats[name]), name
     assert abs(s["dissipation"] - stats["dissipation"]) <= 1e-5 * stats["dissipation"]
     assert abs(o.total_energy(W) - float(g["ke"])) <= 1e-13 * float(g["ke"])
