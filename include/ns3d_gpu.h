@@ -259,6 +259,30 @@ ns3d_status ns3d_total_energy(ns3d_ctx *ctx, double *etot);
 /* compute_energy_spectrum (EnergySpectrum.cpp:62-125): E(k), k = 0..nbins-1,
  * nbins <= 2*global_nx + 1; transform of u,v,w scaled by 1/N, shells by floor(|k|). */
 ns3d_status ns3d_energy_spectrum(ns3d_ctx *ctx, double *Ek, int nbins);
+/* ---- field I/O in the reference's Tecplot ASCII format (host code) -------- */
+/* write_tecplot_field (output.cpp:21-87) of host arrays (interior layout): the
+ * TITLE / VARIABLES / ZONE lines and one "X Y Z rho u v w E p T" record per cell,
+ * x fastest, %.8e, byte-identical to the reference's file for the same state; E and
+ * T as primitiveToConserved computes them. `rank` labels the title and zone as the
+ * reference's per-rank files do. NS3D_ERR_FILE when the file cannot be written. */
+ns3d_status ns3d_tecplot_write(const ns3d_params *p, const double *rho, const double *u,
+                               const double *v, const double *w, const double *pres,
+                               const char *path, double time, int rank);
+/* initialize_from_tecplot (initialization.cpp:35-100) into host arrays: the records
+ * after the first ZONE line as a whitespace-separated stream; E and T are dropped
+ * (the reference rebuilds them from the primitives, main.cpp:70-71). NS3D_ERR_FILE
+ * when the file cannot be opened or holds fewer records than cells. */
+ns3d_status ns3d_tecplot_read(const ns3d_params *p, const char *path, double *rho, double *u,
+                              double *v, double *w, double *pres);
+/* initialize_from_tecplot_downsample (initialization.cpp:102-198): nearest-neighbour
+ * sampling (llround(g * src / n), clamped) of a src_nx x src_ny x src_nz file. */
+ns3d_status ns3d_tecplot_read_downsample(const ns3d_params *p, const char *path, int src_nx,
+                                         int src_ny, int src_nz, double *rho, double *u,
+                                         double *v, double *w, double *pres);
+/* The same for the context's state: download + write, read + upload. */
+ns3d_status ns3d_write_tecplot(ns3d_ctx *ctx, const char *path, double time);
+ns3d_status ns3d_read_tecplot(ns3d_ctx *ctx, const char *path);
+
 /* init_isotropic_turbulence (isotropic_ini.cpp:146-193) with generate_full_turbulence
  * (:25-122) into the context's state: a random-phase solenoidal velocity with spectrum
  * ~ kk exp(-2 kk / k0^2), the phases drawn from mt19937_64(seed) + uniform [0, 1) in the

@@ -52,6 +52,11 @@ _SIGS = {
     "ns3d_energy_spectrum": (_i, [_vp, _D, _i]),
     "ns3d_turbulence_stats": (_i, [_vp, _vp]),
     "ns3d_init_isotropic": (_i, [_vp, _i, ctypes.c_double, ctypes.c_ulonglong, ctypes.c_double]),
+    "ns3d_tecplot_write": (_i, [_vp, _D, _D, _D, _D, _D, ctypes.c_char_p, ctypes.c_double, _i]),
+    "ns3d_tecplot_read": (_i, [_vp, ctypes.c_char_p, _D, _D, _D, _D, _D]),
+    "ns3d_tecplot_read_downsample": (_i, [_vp, ctypes.c_char_p, _i, _i, _i, _D, _D, _D, _D, _D]),
+    "ns3d_write_tecplot": (_i, [_vp, ctypes.c_char_p, ctypes.c_double]),
+    "ns3d_read_tecplot": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_get_stream": (_i, [_vp, _pvp]),
     "ns3d_profile": (_i, [_vp, _i]),
     "ns3d_profile_read": (_i, [_vp, _D, ctypes.POINTER(ctypes.c_longlong)]),

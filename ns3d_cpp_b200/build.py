@@ -48,6 +48,7 @@ UNITS = {
     "ns3d_noalloc.cu": ["--fmad=false"],
     "ns3d_adjoint.cu": ["--fmad=true"],
     "ns3d_params.cpp": [],
+    "ns3d_io.cpp": [],
 }
 
 

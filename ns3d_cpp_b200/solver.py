@@ -318,6 +318,14 @@ class Solver:
         self._ck(self.lib.ns3d_turbulence_stats(self.ctx, ctypes.byref(s)))
         return {n: getattr(s, n) for n, _ in TurbStats._fields_}
 
+    def write_tecplot(self, path: str, time: float = 0.0) -> None:
+        """write_tecplot_field (output.cpp:21-87) of the state to `path`."""
+        self._ck(self.lib.ns3d_write_tecplot(self.ctx, path.encode(), float(time)))
+
+    def read_tecplot(self, path: str) -> None:
+        """initialize_from_tecplot (initialization.cpp:35-100) into the state."""
+        self._ck(self.lib.ns3d_read_tecplot(self.ctx, path.encode()))
+
     def init_isotropic(self, k0: int = 8, A: float = 0.00013, seed: int = 123,
                        mach_t: float = 0.0) -> None:
         """init_isotropic_turbulence (isotropic_ini.cpp:146-193) on the device: the

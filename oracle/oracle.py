@@ -296,6 +296,9 @@ def _ref_lib(path=REF_SO):
         lib.ref_total_energy.restype = ctypes.c_double
         lib.ref_isotropic_post.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
         lib.ref_init_isotropic.argtypes = [ctypes.c_void_p]
+        lib.ref_write_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
+        lib.ref_read_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int]
         _REF[path] = lib
     return _REF[path]
 
@@ -405,6 +408,20 @@ class Ref:
 
     def init_isotropic(self):
         self._check(self.lib.ref_init_isotropic(self.h))
+
+    def write_tecplot(self, directory: str, time: float) -> str:
+        """write_tecplot_field under `directory`; returns the file's path."""
+        self._check(self.lib.ref_write_tecplot(self.h, directory.encode(), float(time)))
+        return os.path.join(directory, "output", f"time_{int(time * 100000)}", "field_rank0.dat")
+
+    def read_tecplot(self, path: str, src=None) -> int:
+        """initialize_from_tecplot[_downsample] + boundary + primitiveToConserved;
+        returns 0, or 1 when the reference's reader reported failure."""
+        sx, sy, sz = src if src else (0, 0, 0)
+        r = self.lib.ref_read_tecplot(self.h, path.encode(), sx, sy, sz)
+        if r < 0:
+            self._check(r)
+        return r
 
 
 # --------------------------------------------------------------------------

@@ -267,6 +267,34 @@ int ref_isotropic_post(void *h, const char *workdir, double t) {
 
 // The reference's isotropic generator (isotropic_ini.cpp:132, k0=8, A=1.3e-4,
 // mt19937_64 seed 123) followed by main.cpp:70-71.
+// write_tecplot_field with `dir` as the working directory (the reference writes
+// output/time_<100000 t>/field_rank0.dat under it).
+int ref_write_tecplot(void *h, const char *dir, double time) {
+    auto *c = static_cast<RefCtx *>(h);
+    char old[4096];
+    if (!getcwd(old, sizeof old) || chdir(dir) != 0) return -1;
+    int r = guarded(c, [&] { write_tecplot_field(c->F, c->G, c->C, c->P, time); });
+    if (chdir(old) != 0) return -1;
+    return r;
+}
+
+// main.cpp:67-71: initialize_from_tecplot (or the downsampling form when
+// src_nx > 0), apply_boundary, primitiveToConserved.
+int ref_read_tecplot(void *h, const char *path, int src_nx, int src_ny, int src_nz) {
+    auto *c = static_cast<RefCtx *>(h);
+    int ok = 1;
+    int r = guarded(c, [&] {
+        ok = src_nx > 0 ? initialize_from_tecplot_downsample(c->F, c->G, c->C, c->P, path, src_nx,
+                                                             src_ny, src_nz)
+                        : initialize_from_tecplot(c->F, c->G, c->C, c->P, path);
+        if (ok) {
+            apply_boundary(c->F, c->G, c->C, c->P);
+            c->F.primitiveToConserved(c->P);
+        }
+    });
+    return r != 0 ? r : (ok ? 0 : 1);
+}
+
 int ref_init_isotropic(void *h) {
     auto *c = static_cast<RefCtx *>(h);
     return guarded(c, [&] {
