@@ -190,13 +190,16 @@ def kernel_bytes_per_cell(cls: str, rsize: int) -> float:
         return w + 5 * rsize
     if cls in ("sweep_y", "sweep_z"):
         return w + 10 * rsize
+    # viscous flux values per cell: 9 in the FP64 form; 12 in the FP32 form
+    # (three float4 blocks, one per differentiated direction)
+    fv = 12 if rsize == 4 else 9
     if cls == "visc_flux":
-        return 4 * 8 + 9 * rsize
+        return 4 * 8 + fv * rsize
     if cls == "update":
         # current + recorded state (stage 1 reads only the recorded one: the
-        # mean over the three stages is 5/3 state reads), T_acc, the 9 viscous
-        # flux blocks, 6 doubles written
-        return (5.0 / 3.0) * w + 5 * rsize + 9 * rsize + 6 * 8
+        # mean over the three stages is 5/3 state reads), T_acc, the viscous
+        # flux values, 6 doubles written
+        return (5.0 / 3.0) * w + 5 * rsize + fv * rsize + 6 * 8
     return 0.0
 
 
