@@ -48,6 +48,13 @@ __device__ __forceinline__ R get_mu(R T, R mu_ref, R S) {
     return mu_ref * pow(T, R(1.5)) * (R(1.0) + S) / (T + S);
 }
 
+// FP32-stencil form: T^1.5 as T sqrt(T) (the difference from pow is far below
+// the float rounding this form carries; pow costs several times more).
+template <>
+__device__ __forceinline__ float get_mu<float>(float T, float mu_ref, float S) {
+    return mu_ref * (T * sqrtf(T)) * (1.0f + S) / (T + S);
+}
+
 // primitiveToConserved (field_structures.h:430-451) for one cell: E and c.
 template <class R>
 __device__ __forceinline__ void p2c_Ec(R rr, R u, R v, R w, R p, R gamma, R& E, R& c) {

@@ -574,15 +574,22 @@ k_visc_flux(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict
 // plane instead of 12 or more. Per cell the arithmetic is the same as in
 // k_visc_flux / k_update (same values, same order).
 // ---------------------------------------------------------------------------
-constexpr int VT_X = 32, VT_Y = 8, VT_H = 4;
-constexpr int VT_SX = VT_X + 2 * VT_H, VT_SY = VT_Y + 2 * VT_H;
+// Tile shape per compute type. FP32: 32 x 16 (halo loads 1.9x the outputs),
+// at most 64 registers and 2 blocks of 512 threads per SM (68 registers and
+// fewer blocks measured 14% slower). FP64: 32 x 8, 128 registers, 2 blocks of
+// 256 threads (a 32 x 16 tile would leave one block per SM).
+template <class R>
+struct VTile {
+    static constexpr int X = 32, Y = sizeof(R) == 4 ? 16 : 8, H = 4;
+    static constexpr int SX = X + 2 * H, SY = Y + 2 * H;
+};
 
-// (FP32: at most 64 registers, 4 blocks of 256 threads per SM; 68 registers
-// and 3 blocks measured 14% slower. FP64: 128 registers, 2 blocks.)
 template <class R, int ORD>
-__global__ void __launch_bounds__(VT_X * VT_Y, sizeof(R) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(VTile<R>::X * VTile<R>::Y, 2)
 k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict__ ctrl,
                 int zb) {
+    constexpr int VT_X = VTile<R>::X, VT_Y = VTile<R>::Y, VT_H = VTile<R>::H;
+    constexpr int VT_SX = VTile<R>::SX, VT_SY = VTile<R>::SY;
     if (ctrl && ctrl->stop) return;
     // FP32-stencil form: values enter the tile and the z queue as float
     // deviations from one reference per block and variable (formed in

@@ -109,32 +109,35 @@ cudaError_t launch_sweep(const LaunchCfg& L, int dir, StateView W, R* tacc, cons
 }
 
 namespace detail {
+template <class R>
 inline bool tiles_25d(const LaunchCfg& L, int bit) {
-    return (L.tiled & bit) && L.zb >= 0 && L.P.nx % VT_X == 0 && L.P.ny % VT_Y == 0;
+    return (L.tiled & bit) && L.zb >= 0 && L.P.nx % VTile<R>::X == 0 && L.P.ny % VTile<R>::Y == 0;
 }
 // Planes per block of the 2.5-D kernels: L.zb when set, else 16 halved until
 // the grid has at least 4 blocks per SM (32^3: 1 plane, 128^3: 8, 256^3: 16).
+template <class R>
 inline int zb_for(const LaunchCfg& L) {
     if (L.zb > 0) return L.zb;
-    const long long tiles = (long long)(L.P.nx / VT_X) * (L.P.ny / VT_Y);
+    const long long tiles = (long long)(L.P.nx / VTile<R>::X) * (L.P.ny / VTile<R>::Y);
     int zb = 16;
     while (zb > 1 && tiles * ((L.P.nz + zb - 1) / zb) < 4 * 148) zb >>= 1;
     return zb;
 }
+template <class R>
 inline dim3 grid_25d(const LaunchCfg& L) {
-    const int zb = zb_for(L);
-    return dim3(L.P.nx / VT_X, L.P.ny / VT_Y, (L.P.nz + zb - 1) / zb);
+    const int zb = zb_for<R>(L);
+    return dim3(L.P.nx / VTile<R>::X, L.P.ny / VTile<R>::Y, (L.P.nz + zb - 1) / zb);
 }
 }  // namespace detail
 
 template <class R>
 cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl) {
-    if (detail::tiles_25d(L, 1)) {
-        const dim3 g = detail::grid_25d(L), b(VT_X, VT_Y);
+    if (detail::tiles_25d<R>(L, 1)) {
+        const dim3 g = detail::grid_25d<R>(L), b(VTile<R>::X, VTile<R>::Y);
         switch (L.P.vis_order) {
-        case 4: k_visc_flux_25d<R, 4><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for(L)); break;
-        case 6: k_visc_flux_25d<R, 6><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for(L)); break;
-        default: k_visc_flux_25d<R, 8><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for(L)); break;
+        case 4: k_visc_flux_25d<R, 4><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for<R>(L)); break;
+        case 6: k_visc_flux_25d<R, 6><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for<R>(L)); break;
+        default: k_visc_flux_25d<R, 8><<<g, b, 0, L.stream>>>(L.P, W, fv, ctrl, detail::zb_for<R>(L)); break;
         }
         return cudaGetLastError();
     }
