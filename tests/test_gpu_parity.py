@@ -178,6 +178,27 @@ def test_reductions_match_oracle(oracle_mod):
     assert abs(st["mach_t"] - 0.3) < 1e-12
 
 
+def test_fp32_tiled_viscous_box_close_to_fp64(oracle_mod):
+    """The FP32 form on a box that takes the tiled viscous kernel (nx % 32 == 0,
+    ny % 16 == 0) and the warp-per-row x sweep, against the FP64 oracle with the
+    tolerances of test_fp32_stencils_close_to_fp64."""
+    nz, ny, nx = 8, 16, 32
+    cfg = ref_cfg(nx)
+    cfg.update(global_ny=ny, global_nz=nz)
+    W = np.ascontiguousarray(tgv_input(nx, seed=12)[:, :nz, :ny, :])
+    o = oracle_mod.Oracle(cfg)
+    with ns.Solver(params_from_cfg(cfg, precision="fp32acc64")) as s:
+        s.upload_primitive(W)
+        rhs = s.compute_rhs()
+        s.step(10)
+        Wg = s.download_primitive()
+    assert np.all(relerr(rhs, o.rhs(W)) <= 5e-5), relerr(rhs, o.rhs(W))
+    Wo = W
+    for _ in range(10):
+        Wo, _, st = o.cfl_step(Wo)
+    assert np.all(relerr(Wg, Wo) <= 1e-5)
+
+
 def test_init_isotropic_matches_reference_golden():
     """init_isotropic_turbulence on the device (cuFFT) against the reference's
     own field (tests/golden/isotropic_ic.npz, generated by its FFTW-API build
