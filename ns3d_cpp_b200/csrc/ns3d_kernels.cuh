@@ -427,15 +427,21 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     double raw[5], nxt[5];
     load_raw(nch - 1, raw);
     split_raw(raw, lastp, lastm);
-    load_raw(0, raw);
-    split_raw(raw, firstp, firstm);
+    if (nch > 1) {
+        load_raw(0, raw);
+        split_raw(raw, firstp, firstm);
+    } else {  // one chunk per row: the first chunk is the last
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { firstp[q] = lastp[q]; firstm[q] = lastm[q]; }
+    }
     put(0, lastp, lastm);
     put(1, firstp, firstm);
     if (nch > 1) load_raw(1, nxt);
     __syncwarp();
-    // the face on the -x side of cell 0 (face nx-1 by periodicity)
-    R carry[5];
-    face_at(1, -1, 0, carry);
+    // the face on the -x side of cell 0 (face nx-1 by periodicity); with one
+    // chunk per row it is lane 31's own face, taken by shuffle below
+    R carry[5] = {R(0), R(0), R(0), R(0), R(0)};
+    if (nch > 1) face_at(1, -1, 0, carry);
     int cur = 1;
     for (int c = 0; c < nch; ++c) {
         const int nslot = cur == 2 ? 0 : cur + 1;
@@ -459,8 +465,9 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             R left = __shfl_up_sync(0xffffffffu, face[q], 1);
-            if (lane == 0) left = carry[q];
-            carry[q] = __shfl_sync(0xffffffffu, face[q], 31);
+            const R last = __shfl_sync(0xffffffffu, face[q], 31);
+            if (lane == 0) left = nch == 1 ? last : carry[q];
+            carry[q] = last;
             const R d = face[q] - left;
             tacc[q * n + id] = d * inv_h;
         }
