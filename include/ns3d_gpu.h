@@ -279,9 +279,19 @@ ns3d_status ns3d_tecplot_read(const ns3d_params *p, const char *path, double *rh
 ns3d_status ns3d_tecplot_read_downsample(const ns3d_params *p, const char *path, int src_nx,
                                          int src_ny, int src_nz, double *rho, double *u,
                                          double *v, double *w, double *pres);
+/* write_residuals_tecplot (output.cpp:92-128): `path` is created with its TITLE /
+ * VARIABLES header when step == 1 and appended to otherwise; one row
+ * "step res_rho res_rhou res_rhov res_rhow res_E Etot" (%.8e). */
+ns3d_status ns3d_residuals_write(const char *path, int step, const double *res, double etot);
 /* The same for the context's state: download + write, read + upload. */
 ns3d_status ns3d_write_tecplot(ns3d_ctx *ctx, const char *path, double time);
 ns3d_status ns3d_read_tecplot(ns3d_ctx *ctx, const char *path);
+
+/* compute_diagnostics (postprocess.cpp:7-98) after a step: res[q] = sqrt(sum (U - U0)^2
+ * dx^3) / max |U| for rho, rhou, rhov, rhow, E, with U the current state and U0 the
+ * recorded one (recordConservedTo0 of the step's start; stepping keeps it until the
+ * next step). */
+ns3d_status ns3d_residuals(ns3d_ctx *ctx, double *res);
 
 /* init_isotropic_turbulence (isotropic_ini.cpp:146-193) with generate_full_turbulence
  * (:25-122) into the context's state: a random-phase solenoidal velocity with spectrum

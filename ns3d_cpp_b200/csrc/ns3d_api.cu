@@ -258,6 +258,59 @@ __global__ void k_iso_scale(long long n, double s, StateOut W) {
     W.w[id] *= s;
 }
 
+// ---- residual monitor (compute_diagnostics, postprocess.cpp:7-98)
+
+// Per block: sum over cells of (U - U0)^2 dx^3 and max |U| for the five
+// conserved variables (U of the current state, U0 of the recorded one, both as
+// primitiveToConserved computes them). part[block * 10 + q]: sums q = 0..4,
+// maxima 5..9.
+__global__ void __launch_bounds__(256)
+k_resid_partial(DevParams P, StateView Wc, StateView W0, double* __restrict__ part) {
+    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, m[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double dx3 = P.dx * P.dx * P.dx;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < P.n;
+         id += (long long)gridDim.x * blockDim.x) {
+        double U[5], U0[5];
+        prim2cons_cell(Wc, id, P.gamma, U);
+        prim2cons_cell(W0, id, P.gamma, U0);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double r = U[q] - U0[q];
+            s[q] += r * r * dx3;
+            m[q] = fmax(m[q], fabs(U[q]));
+        }
+    }
+    __shared__ double red[10][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 10; ++q) {
+        double x = q < 5 ? s[q] : m[q - 5];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = q < 5 ? x + y : fmax(x, y);
+        }
+        if (lane == 0) red[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 10) {
+        const int q = threadIdx.x;
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            x = q < 5 ? x + red[q][w] : fmax(x, red[q][w]);
+        part[(long long)blockIdx.x * 10 + q] = x;
+    }
+}
+
+__global__ void k_resid_final(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
+    const int q = threadIdx.x;
+    if (q >= 10) return;
+    double x = 0.0;
+    for (int b = 0; b < nblocks; ++b)
+        x = q < 5 ? x + part[(long long)b * 10 + q] : fmax(x, part[(long long)b * 10 + q]);
+    out[q] = x;
+}
+
 // conservedToPrimitive (+ T) of an uploaded conserved state held in `U`.
 __global__ void k_cons2prim(DevParams P, const double* __restrict__ U, StateOut W) {
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -935,6 +988,22 @@ ns3d_status ns3d_last_dt(ns3d_ctx* ctx, double* dt) {
     ns3d_status s = read_ctrl(ctx);
     if (s != NS3D_OK) return s;
     *dt = ctx->ctrl_host->dt;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_residuals(ns3d_ctx* ctx, double* res) {
+    if (!ctx || !res) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    static_assert(NSUMS >= 10, "the residual partials share the sums buffers");
+    NS3D_LAUNCH(NS3D_KERNEL_OTHER, 2,
+                (k_resid_partial<<<ctx->sums_blocks, 256, 0, ctx->stream>>>(
+                     ctx->L.P, view(ctx, ctx->cur), view(ctx, ctx->rec), ctx->sums_part),
+                 k_resid_final<<<1, 32, 0, ctx->stream>>>(ctx->sums_part, ctx->sums_blocks,
+                                                          ctx->sums_out)));
+    double h[10];
+    NS3D_CK(cudaMemcpyAsync(h, ctx->sums_out, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < 5; ++q) res[q] = std::sqrt(h[q]) / h[5 + q];
     return NS3D_OK;
 }
 

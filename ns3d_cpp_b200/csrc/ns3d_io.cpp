@@ -257,6 +257,22 @@ ns3d_status ns3d_tecplot_read(const ns3d_params* p, const char* path, double* rh
                                         u, v, w, pres);
 }
 
+ns3d_status ns3d_residuals_write(const char* path, int step, const double* res, double etot) {
+    if (!path || !res) return NS3D_ERR_INVALID;
+    // write_residuals_tecplot (output.cpp:92-128): a new file with its header at
+    // step 1, one appended row per monitored step after that
+    FILE* f = std::fopen(path, step == 1 ? "wb" : "ab");
+    if (!f) return NS3D_ERR_FILE;
+    if (step == 1) {
+        std::fprintf(f, "TITLE = \"Residuals vs Step\"\n");
+        std::fprintf(f, "VARIABLES = \"Step\" \"Res_rho\" \"Res_rhou\" \"Res_rhov\" \"Res_rhow\" "
+                        "\"Res_E\" \"Etot\"\n");
+    }
+    std::fprintf(f, "%d %.8e %.8e %.8e %.8e %.8e %.8e\n", step, res[0], res[1], res[2], res[3],
+                 res[4], etot);
+    return std::fclose(f) == 0 ? NS3D_OK : NS3D_ERR_FILE;
+}
+
 ns3d_status ns3d_write_tecplot(ns3d_ctx* ctx, const char* path, double time) {
     if (!ctx || !path) return NS3D_ERR_INVALID;
     ns3d_params p;

@@ -318,6 +318,13 @@ class Solver:
         self._ck(self.lib.ns3d_turbulence_stats(self.ctx, ctypes.byref(s)))
         return {n: getattr(s, n) for n, _ in TurbStats._fields_}
 
+    def residuals(self) -> np.ndarray:
+        """compute_diagnostics (postprocess.cpp:7-98) after a step: the five
+        normalised L2 residuals of rho, rhou, rhov, rhow, E."""
+        out = np.zeros(5)
+        self._ck(self.lib.ns3d_residuals(self.ctx, _dptr(out)))
+        return out
+
     def write_tecplot(self, path: str, time: float = 0.0) -> None:
         """write_tecplot_field (output.cpp:21-87) of the state to `path`."""
         self._ck(self.lib.ns3d_write_tecplot(self.ctx, path.encode(), float(time)))

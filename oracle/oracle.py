@@ -296,6 +296,9 @@ def _ref_lib(path=REF_SO):
         lib.ref_total_energy.restype = ctypes.c_double
         lib.ref_isotropic_post.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
         lib.ref_init_isotropic.argtypes = [ctypes.c_void_p]
+        lib.ref_diagnostics.argtypes = [ctypes.c_void_p, D]
+        lib.ref_write_residuals.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                            ctypes.c_int]
         lib.ref_write_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
         lib.ref_read_tecplot.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int]
@@ -409,6 +412,18 @@ class Ref:
     def init_isotropic(self):
         self._check(self.lib.ref_init_isotropic(self.h))
 
+    def diagnostics(self) -> np.ndarray:
+        """compute_diagnostics: the five residuals of the last step."""
+        out = np.zeros(5)
+        self._check(self.lib.ref_diagnostics(self.h, _dp(out)))
+        return out
+
+    def write_residuals(self, directory: str, step: int, energy: bool = True) -> str:
+        """write_residuals_tecplot under `directory`; returns the file's path."""
+        self._check(self.lib.ref_write_residuals(self.h, directory.encode(), int(step),
+                                                 int(bool(energy))))
+        return os.path.join(directory, "output", "output_residuals.dat")
+
     def write_tecplot(self, directory: str, time: float) -> str:
         """write_tecplot_field under `directory`; returns the file's path."""
         self._check(self.lib.ref_write_tecplot(self.h, directory.encode(), float(time)))
@@ -449,6 +464,26 @@ def spectrum(u, v, w):
     kk = np.floor(np.sqrt(K1 * K1 + K2 * K2 + K3 * K3)).astype(np.int64)
     Ek = np.bincount(kk.ravel(), weights=e.ravel(), minlength=2 * nx + 1)
     return Ek[: 2 * nx + 1]
+
+
+def residuals(U, U0, dx: float) -> np.ndarray:
+    """compute_diagnostics (postprocess.cpp:7-98) from the conserved state U
+    after a step and U0 at its start, both (5, nz, ny, nx): sqrt(sum (U - U0)^2
+    dx^3) / max |U| per variable. The sums run in the reference's order (x
+    fastest, one running total; np.cumsum is sequential), so single-rank results
+    are bit-identical."""
+    dx3 = dx * dx * dx
+    out = np.empty(5)
+    for q in range(5):
+        r = (U[q] - U0[q]).ravel()
+        s = np.cumsum(r * r * dx3)[-1]
+        out[q] = np.sqrt(s) / np.max(np.abs(U[q]))
+    return out
+
+
+def residuals_row(step: int, res, etot: float) -> str:
+    """One row of write_residuals_tecplot (output.cpp:124-126)."""
+    return f"{step} " + " ".join(f"{x:.8e}" for x in list(res) + [etot]) + "\n"
 
 
 def turbulence_stats(sums: np.ndarray, Ek: np.ndarray, N: int, gamma: float, Rgas: float):

@@ -295,6 +295,33 @@ int ref_read_tecplot(void *h, const char *path, int src_nx, int src_ny, int src_
     return r != 0 ? r : (ok ? 0 : 1);
 }
 
+// compute_diagnostics (postprocess.cpp:7-98) on the state left by the last step
+// (U0 recorded at its start); out = global_res_rho, _rhou, _rhov, _rhow, _E.
+int ref_diagnostics(void *h, double *out) {
+    auto *c = static_cast<RefCtx *>(h);
+    return guarded(c, [&] {
+        compute_diagnostics(c->F, c->P, c->G);
+        const double r[5] = {c->F.global_res_rho, c->F.global_res_rhou, c->F.global_res_rhov,
+                             c->F.global_res_rhow, c->F.global_res_E};
+        for (int q = 0; q < 5; ++q) out[q] = r[q];
+    });
+}
+
+// write_residuals_tecplot (output.cpp:92-128) with `dir` as the working
+// directory: output/output_residuals.dat, the row of the last diagnostics and
+// of F.global_Etot (compute_total_energy first when `energy` is set).
+int ref_write_residuals(void *h, const char *dir, int step, int energy) {
+    auto *c = static_cast<RefCtx *>(h);
+    char old[4096];
+    if (!getcwd(old, sizeof old) || chdir(dir) != 0) return -1;
+    int r = guarded(c, [&] {
+        if (energy) compute_total_energy(c->F, c->G, c->C, c->P);
+        write_residuals_tecplot(c->F, step, "output_residuals.dat");
+    });
+    if (chdir(old) != 0) return -1;
+    return r;
+}
+
 int ref_init_isotropic(void *h) {
     auto *c = static_cast<RefCtx *>(h);
     return guarded(c, [&] {
