@@ -287,6 +287,16 @@ ns3d_status ns3d_residuals_write(const char *path, int step, const double *res, 
 ns3d_status ns3d_write_tecplot(ns3d_ctx *ctx, const char *path, double time);
 ns3d_status ns3d_read_tecplot(ns3d_ctx *ctx, const char *path);
 
+/* Binary checkpoint of the context (no counterpart in the reference, which restarts
+ * from its 9-digit Tecplot field, initialization.cpp:35-100): the current state's
+ * rho, u, v, w, p, T bit for bit, the clock of ns3d_time_advance and the state's CFL
+ * minimum, with a 64-bit checksum. Reading it into a context of the same grid gives a
+ * run that repeats the uninterrupted one exactly (U0 recorded from the read state).
+ * NS3D_ERR_FILE: unreadable, not a checkpoint, truncated or checksum mismatch;
+ * NS3D_ERR_INVALID: another grid. */
+ns3d_status ns3d_checkpoint_write(ns3d_ctx *ctx, const char *path);
+ns3d_status ns3d_checkpoint_read(ns3d_ctx *ctx, const char *path);
+
 /* compute_diagnostics (postprocess.cpp:7-98) after a step: res[q] = sqrt(sum (U - U0)^2
  * dx^3) / max |U| for rho, rhou, rhov, rhow, E, with U the current state and U0 the
  * recorded one (recordConservedTo0 of the step's start; stepping keeps it until the

@@ -57,6 +57,8 @@ _SIGS = {
     "ns3d_tecplot_read_downsample": (_i, [_vp, ctypes.c_char_p, _i, _i, _i, _D, _D, _D, _D, _D]),
     "ns3d_write_tecplot": (_i, [_vp, ctypes.c_char_p, ctypes.c_double]),
     "ns3d_residuals": (_i, [_vp, _D]),
+    "ns3d_checkpoint_write": (_i, [_vp, ctypes.c_char_p]),
+    "ns3d_checkpoint_read": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_residuals_write": (_i, [ctypes.c_char_p, _i, _D, ctypes.c_double]),
     "ns3d_read_tecplot": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_get_stream": (_i, [_vp, _pvp]),

@@ -8,9 +8,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ns3d_gpu.h"
@@ -1004,6 +1006,132 @@ ns3d_status ns3d_residuals(ns3d_ctx* ctx, double* res) {
     NS3D_CK(cudaMemcpyAsync(h, ctx->sums_out, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     NS3D_CK(cudaStreamSynchronize(ctx->stream));
     for (int q = 0; q < 5; ++q) res[q] = std::sqrt(h[q]) / h[5 + q];
+    return NS3D_OK;
+}
+
+// ---- binary checkpoint
+//
+// The reference restarts from its Tecplot field (9 significant digits). The
+// checkpoint keeps the current state buffer's six arrays (rho, u, v, w, p, T)
+// bit for bit, the clock (time, next output time) and the CFL minimum of the
+// state, so a run continued from it repeats the uninterrupted run exactly.
+// Layout: a 96-byte header (CkptHeader, little-endian), then the six arrays of
+// nx*ny*nz doubles each, x fastest.
+
+namespace {
+
+struct CkptHeader {
+    char magic[8];               // "NS3DCKPT"
+    uint32_t version, header_bytes;
+    int32_t nx, ny, nz, precision;
+    double time, out_next;
+    uint64_t dtmin_bits;         // the CFL minimum's bit pattern when dtmin_valid
+    uint32_t dtmin_valid, reserved;
+    double dx, dy, dz;
+    uint64_t payload_hash;       // hash_words over the six arrays
+};
+static_assert(sizeof(CkptHeader) == 96, "checkpoint header layout");
+constexpr char kCkptMagic[8] = {'N', 'S', '3', 'D', 'C', 'K', 'P', 'T'};
+constexpr uint32_t kCkptVersion = 1;
+
+// FNV-1a over 64-bit words: chunks of 2^17 words hashed on the host's threads,
+// the chunk hashes folded in order, so the value does not depend on the
+// thread count.
+uint64_t hash_words(const uint64_t* w, long long n) {
+    constexpr uint64_t kOffset = 0xcbf29ce484222325ull, kPrime = 0x100000001b3ull;
+    constexpr long long C = 1ll << 17;
+    const long long nch = (n + C - 1) / C;
+    std::vector<uint64_t> hs((size_t)nch);
+    const long long hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::max(1ll, std::min({nch, hw, 64ll}));
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t)
+        th.emplace_back([&, t] {
+            for (long long c = t; c < nch; c += T) {
+                uint64_t h = kOffset;
+                const long long e = std::min(n, (c + 1) * C);
+                for (long long i = c * C; i < e; ++i) h = (h ^ w[i]) * kPrime;
+                hs[(size_t)c] = h;
+            }
+        });
+    for (auto& x : th) x.join();
+    uint64_t h = kOffset;
+    for (uint64_t x : hs) h = (h ^ x) * kPrime;
+    return h;
+}
+
+bool same_bits(double a, double b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+}  // namespace
+
+ns3d_status ns3d_checkpoint_write(ns3d_ctx* ctx, const char* path) {
+    if (!ctx || !path) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    CkptHeader h{};
+    std::memcpy(h.magic, kCkptMagic, sizeof h.magic);
+    h.version = kCkptVersion;
+    h.header_bytes = sizeof h;
+    h.nx = ctx->p.global_nx;
+    h.ny = ctx->p.global_ny;
+    h.nz = ctx->p.global_nz;
+    h.precision = ctx->p.precision;
+    h.time = ctx->time;
+    h.out_next = ctx->out_next;
+    h.dtmin_valid = ctx->dtmin_valid ? 1u : 0u;
+    h.dx = ctx->p.dx;
+    h.dy = ctx->p.dy;
+    h.dz = ctx->p.dz;
+    const long long nw = 6 * ctx->n;
+    std::vector<double> buf((size_t)nw);
+    if (ctx->dtmin_valid)
+        NS3D_CK(cudaMemcpyAsync(&h.dtmin_bits, &ctx->ctrl->dtmin_bits, sizeof h.dtmin_bits,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    NS3D_CK(cudaMemcpyAsync(buf.data(), warr(ctx, ctx->cur, 0), sizeof(double) * nw,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    h.payload_hash = hash_words(reinterpret_cast<const uint64_t*>(buf.data()), nw);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, NS3D_ERR_FILE, std::string("cannot open ") + path);
+    bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
+              std::fwrite(buf.data(), sizeof(double), (size_t)nw, f) == (size_t)nw;
+    ok = std::fclose(f) == 0 && ok;
+    return ok ? NS3D_OK : fail(ctx, NS3D_ERR_FILE, std::string("write failed: ") + path);
+}
+
+ns3d_status ns3d_checkpoint_read(ns3d_ctx* ctx, const char* path) {
+    if (!ctx || !path) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, NS3D_ERR_FILE, std::string("cannot open ") + path);
+    CkptHeader h{};
+    if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, kCkptMagic, sizeof h.magic) ||
+        h.version != kCkptVersion || h.header_bytes != sizeof h) {
+        std::fclose(f);
+        return fail(ctx, NS3D_ERR_FILE, std::string("not a version 1 checkpoint: ") + path);
+    }
+    if (h.nx != ctx->p.global_nx || h.ny != ctx->p.global_ny || h.nz != ctx->p.global_nz ||
+        !same_bits(h.dx, ctx->p.dx) || !same_bits(h.dy, ctx->p.dy) || !same_bits(h.dz, ctx->p.dz)) {
+        std::fclose(f);
+        return fail(ctx, NS3D_ERR_INVALID, "the checkpoint's grid differs from the context's");
+    }
+    const long long nw = 6 * ctx->n;
+    std::vector<double> buf((size_t)nw);
+    const size_t got = std::fread(buf.data(), sizeof(double), (size_t)nw, f);
+    std::fclose(f);
+    if (got != (size_t)nw) return fail(ctx, NS3D_ERR_FILE, std::string("truncated checkpoint: ") + path);
+    if (hash_words(reinterpret_cast<const uint64_t*>(buf.data()), nw) != h.payload_hash)
+        return fail(ctx, NS3D_ERR_FILE, std::string("checkpoint checksum mismatch: ") + path);
+    NS3D_CK(cudaMemcpyAsync(warr(ctx, ctx->cur, 0), buf.data(), sizeof(double) * nw,
+                            cudaMemcpyHostToDevice, ctx->stream));
+    // the CFL minimum only carries over between contexts of the same form
+    ctx->dtmin_valid = h.dtmin_valid != 0 && h.precision == ctx->p.precision;
+    if (ctx->dtmin_valid)
+        NS3D_CK(cudaMemcpyAsync(&ctx->ctrl->dtmin_bits, &h.dtmin_bits, sizeof h.dtmin_bits,
+                                cudaMemcpyHostToDevice, ctx->stream));
+    NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    ctx->rec = ctx->cur;
+    ctx->time = h.time;
+    ctx->out_next = h.out_next;
     return NS3D_OK;
 }
 

@@ -325,6 +325,14 @@ class Solver:
         self._ck(self.lib.ns3d_residuals(self.ctx, _dptr(out)))
         return out
 
+    def checkpoint_write(self, path: str) -> None:
+        """The state, clock and CFL minimum, bit for bit (a binary restart file)."""
+        self._ck(self.lib.ns3d_checkpoint_write(self.ctx, path.encode()))
+
+    def checkpoint_read(self, path: str) -> None:
+        """Continue from a checkpoint_write file of the same grid."""
+        self._ck(self.lib.ns3d_checkpoint_read(self.ctx, path.encode()))
+
     def write_tecplot(self, path: str, time: float = 0.0) -> None:
         """write_tecplot_field (output.cpp:21-87) of the state to `path`."""
         self._ck(self.lib.ns3d_write_tecplot(self.ctx, path.encode(), float(time)))
