@@ -179,6 +179,14 @@ ns3d_status ns3d_runge_kutta_3(ns3d_ctx *ctx, double dt);
 ns3d_status ns3d_time_advance(ns3d_ctx *ctx, int max_steps, double *time, int *steps_done);
 /* `nsteps` RK3 steps with a CFL (or fixed) dt each, no clipping: the bench step. */
 ns3d_status ns3d_step(ns3d_ctx *ctx, int nsteps);
+/* The same loop as ns3d_time_advance, also ending right after a step whose if_output
+ * is set (maincycle.cpp:33-45), so that a monitor can write that step's output; the
+ * next call continues the loop. *events: NS3D_EVENT_OUTPUT when the last completed
+ * step is an output step, NS3D_EVENT_END when the loop reached TotalTime. */
+#define NS3D_EVENT_OUTPUT 1
+#define NS3D_EVENT_END 2
+ns3d_status ns3d_time_advance_segment(ns3d_ctx *ctx, int max_steps, double *time, int *steps_done,
+                                      int *events);
 /* dt of the last step taken on the device. */
 ns3d_status ns3d_last_dt(ns3d_ctx *ctx, double *dt);
 
@@ -318,6 +326,30 @@ ns3d_status ns3d_init_isotropic(ns3d_ctx *ctx, int k0, double A, unsigned long l
 /* compute_turbulence_statistics (ana_isotropic.cpp:196-314): every quantity of its
  * statistics row, without the rank-0 gather and the spectrum file round trip. */
 ns3d_status ns3d_turbulence_stats(ns3d_ctx *ctx, ns3d_turb_stats *out);
+/* The same statistics from a caller's spectrum Ek[0..nbins) (the reference computes
+ * them from the spectrum re-read from its 6-digit file, ana_isotropic.cpp:210-221). */
+ns3d_status ns3d_turbulence_stats_spectrum(ns3d_ctx *ctx, const double *Ek, int nbins,
+                                           ns3d_turb_stats *out);
+
+/* compute_energy_spectrum's file (EnergySpectrum.cpp:127-133): one "k E(k)" row per
+ * bin, E(k) in the stream's default 6-digit format (%g). */
+ns3d_status ns3d_spectrum_write(const char *path, const double *Ek, int nbins);
+/* compute_turbulence_statistics' table (ana_isotropic.cpp:317-342): the header line
+ * when `path` does not exist yet, then one appended row of 12 values (%.8e). */
+ns3d_status ns3d_stats_write(const char *path, double time, const ns3d_turb_stats *s);
+
+/* time_advance (maincycle.cpp:7-112) with its monitor and output, files under
+ * `workdir`/output as the reference writes them under its working directory:
+ * every monitor_Stepfreq-th step and step 1, the residuals (monitor_res; rows of
+ * output_residuals.dat), the total energy (monitor_energy) and the isotropic
+ * post-processing (spectrum file + statistics row); after every output step, the
+ * Tecplot field time_<100000 t>/field_rank0.dat (post_basicfield) and the isotropic
+ * post-processing. verbose: the reference's "[Step n] ..." monitor lines on stdout.
+ * Steps are numbered from 1 in each call. Between monitor and output steps the loop
+ * runs on the device without host synchronisation. NS3D_ERR_INVALID for
+ * monitor_Stepfreq <= 0 (a division by zero in the reference). */
+ns3d_status ns3d_run(ns3d_ctx *ctx, const char *workdir, int max_steps, int verbose,
+                     double *time, int *steps_done);
 
 #ifdef __cplusplus
 }

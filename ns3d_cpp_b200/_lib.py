@@ -57,6 +57,12 @@ _SIGS = {
     "ns3d_tecplot_read_downsample": (_i, [_vp, ctypes.c_char_p, _i, _i, _i, _D, _D, _D, _D, _D]),
     "ns3d_write_tecplot": (_i, [_vp, ctypes.c_char_p, ctypes.c_double]),
     "ns3d_residuals": (_i, [_vp, _D]),
+    "ns3d_time_advance_segment": (_i, [_vp, _i, _D, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    "ns3d_turbulence_stats_spectrum": (_i, [_vp, _D, _i, _vp]),
+    "ns3d_spectrum_write": (_i, [ctypes.c_char_p, _D, _i]),
+    "ns3d_stats_write": (_i, [ctypes.c_char_p, ctypes.c_double, _vp]),
+    "ns3d_run": (_i, [_vp, ctypes.c_char_p, _i, _i, _D, ctypes.POINTER(ctypes.c_int)]),
     "ns3d_checkpoint_write": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_checkpoint_read": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_residuals_write": (_i, [ctypes.c_char_p, _i, _D, ctypes.c_double]),

@@ -8,6 +8,8 @@ Translation units and their floating-point contracts:
   float division/sqrt, denormals flushed.
 * ``ns3d_api.cu``   -- C ABI, transfers, reductions, spectrum; ``-fmad=false``.
 * ``ns3d_params.cpp`` -- solver.in parser (host only).
+* ``ns3d_io.cpp``   -- Tecplot field, residual, spectrum and statistics files (host only).
+* ``ns3d_run.cpp``  -- time_advance with its monitor and output (host only).
 
 Run ``python -m ns3d_cpp_b200.build`` (or ``build()``); objects go to
 ``ns3d_cpp_b200/_build/`` and the library next to this file.
@@ -49,6 +51,7 @@ UNITS = {
     "ns3d_adjoint.cu": ["--fmad=true"],
     "ns3d_params.cpp": [],
     "ns3d_io.cpp": [],
+    "ns3d_run.cpp": [],
 }
 
 

@@ -60,6 +60,7 @@ struct ns3d_ctx {
     int sums_blocks = 0;
     bool dtmin_valid = false;
     double time = 0.0, out_next = 0.0;
+    int last_events = 0;         // NS3D_EVENT_* of the last stepping call
     // spectrum
     cufftHandle fft = 0;
     bool fft_ready = false;
@@ -966,6 +967,10 @@ static ns3d_status run_steps(ns3d_ctx* ctx, int mode, int nsteps, int* steps_don
     ctx->time = h.time;
     ctx->out_next = h.out_next;
     ctx->dtmin_valid = true;
+    // if_output of the last completed step (mode 2 stops right after one), and
+    // whether time_advance's loop has reached TotalTime
+    ctx->last_events = (d > 0 && h.output && !h.stop_in_pre ? NS3D_EVENT_OUTPUT : 0) |
+                       (h.stop && h.stop_reason == STOP_TOTAL_TIME ? NS3D_EVENT_END : 0);
     if (h.stop && h.stop_reason == STOP_NONPHYSICAL) return fail(ctx, NS3D_ERR_NONPHYSICAL, "non-physical state");
     if (h.stop && h.stop_reason == STOP_DT_SMALL) return fail(ctx, NS3D_ERR_DT, "dt too small");
     return NS3D_OK;
@@ -982,6 +987,18 @@ ns3d_status ns3d_time_advance(ns3d_ctx* ctx, int max_steps, double* time, int* s
     ns3d_status s = run_steps(ctx, 1, max_steps, &done);
     if (time) *time = ctx->time;
     if (steps_done) *steps_done = done;
+    return s;
+}
+
+ns3d_status ns3d_time_advance_segment(ns3d_ctx* ctx, int max_steps, double* time,
+                                      int* steps_done, int* events) {
+    if (!ctx || max_steps < 0) return NS3D_ERR_INVALID;
+    int done = 0;
+    ctx->last_events = 0;
+    ns3d_status s = run_steps(ctx, 2, max_steps, &done);
+    if (time) *time = ctx->time;
+    if (steps_done) *steps_done = done;
+    if (events) *events = s == NS3D_OK ? ctx->last_events : 0;
     return s;
 }
 
@@ -1361,14 +1378,12 @@ ns3d_status ns3d_launch_count(const ns3d_ctx* ctx, long long* count) {
     return NS3D_OK;
 }
 
-ns3d_status ns3d_turbulence_stats(ns3d_ctx* ctx, ns3d_turb_stats* out) {
-    if (!ctx || !out) return NS3D_ERR_INVALID;
+// compute_turbulence_statistics (ana_isotropic.cpp:196-314) from the state's
+// sums and the spectrum Ek[0..kmax).
+static ns3d_status stats_from(ns3d_ctx* ctx, const double* Ek, int kmax, ns3d_turb_stats* out) {
     double s[NSUMS];
     ns3d_status st = compute_sums(ctx, s);
     if (st != NS3D_OK) return st;
-    const int kmax = 2 * ctx->p.global_nx + 1;
-    std::vector<double> Ek(kmax);
-    if ((st = ns3d_energy_spectrum(ctx, Ek.data(), kmax)) != NS3D_OK) return st;
     const double N = (double)ctx->n;
     std::memset(out, 0, sizeof(*out));
     out->total_energy = s[0] * (ctx->p.dx * ctx->p.dy * ctx->p.dz);
@@ -1392,6 +1407,21 @@ ns3d_status ns3d_turbulence_stats(ns3d_ctx* ctx, ns3d_turb_stats* out) {
     out->tau_eta = std::pow(out->nu / eps, 0.5);
     out->taylor = std::sqrt(15.0 * out->nu * out->u_rms * out->u_rms / eps);
     return NS3D_OK;
+}
+
+ns3d_status ns3d_turbulence_stats(ns3d_ctx* ctx, ns3d_turb_stats* out) {
+    if (!ctx || !out) return NS3D_ERR_INVALID;
+    const int kmax = 2 * ctx->p.global_nx + 1;
+    std::vector<double> Ek(kmax);
+    ns3d_status st = ns3d_energy_spectrum(ctx, Ek.data(), kmax);
+    if (st != NS3D_OK) return st;
+    return stats_from(ctx, Ek.data(), kmax, out);
+}
+
+ns3d_status ns3d_turbulence_stats_spectrum(ns3d_ctx* ctx, const double* Ek, int nbins,
+                                           ns3d_turb_stats* out) {
+    if (!ctx || !Ek || nbins < 1 || !out) return NS3D_ERR_INVALID;
+    return stats_from(ctx, Ek, nbins, out);
 }
 
 ns3d_status ns3d_init_isotropic(ns3d_ctx* ctx, int k0, double A, unsigned long long seed,

@@ -257,6 +257,31 @@ ns3d_status ns3d_tecplot_read(const ns3d_params* p, const char* path, double* rh
                                         u, v, w, pres);
 }
 
+ns3d_status ns3d_spectrum_write(const char* path, const double* Ek, int nbins) {
+    if (!path || !Ek || nbins < 1) return NS3D_ERR_INVALID;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return NS3D_ERR_FILE;
+    for (int k = 0; k < nbins; ++k) std::fprintf(f, "%d %g\n", k, Ek[k]);
+    return std::fclose(f) == 0 ? NS3D_OK : NS3D_ERR_FILE;
+}
+
+ns3d_status ns3d_stats_write(const char* path, double time, const ns3d_turb_stats* s) {
+    if (!path || !s) return NS3D_ERR_INVALID;
+    FILE* probe = std::fopen(path, "rb");
+    const bool exists = probe != nullptr;
+    if (probe) std::fclose(probe);
+    FILE* f = std::fopen(path, "ab");
+    if (!f) return NS3D_ERR_FILE;
+    if (!exists)
+        std::fprintf(f, "current_time Kinetic Energy TKE u_rms Dissipation Taylor Kol_scale "
+                        "Kol_vel Kol_time Taylor_Li Re_lambda Mach_t\n");
+    const double v[12] = {time,     s->kinetic_energy, s->tke,     s->u_rms,
+                          s->dissipation, s->taylor,   s->eta,     s->u_eta,
+                          s->tau_eta, s->taylor_li,    s->re_lambda, s->mach_t};
+    for (int q = 0; q < 12; ++q) std::fprintf(f, q < 11 ? "%.8e " : "%.8e\n", v[q]);
+    return std::fclose(f) == 0 ? NS3D_OK : NS3D_ERR_FILE;
+}
+
 ns3d_status ns3d_residuals_write(const char* path, int step, const double* res, double etot) {
     if (!path || !res) return NS3D_ERR_INVALID;
     // write_residuals_tecplot (output.cpp:92-128): a new file with its header at

@@ -42,10 +42,11 @@ struct Ctrl {
     int active;                      // a step is in flight
     long long bad_cell;              // first non-physical cell (linear index), or n
     int stop_in_pre;                 // the stop came from the start-of-iteration checks
-    int pad1;
+    int output;                      // if_output of the last iteration begun (maincycle.cpp:33-45)
 };
 
-enum : int { STOP_NONE = 0, STOP_TOTAL_TIME = 1, STOP_DT_SMALL = 2, STOP_NONPHYSICAL = 3 };
+enum : int { STOP_NONE = 0, STOP_TOTAL_TIME = 1, STOP_DT_SMALL = 2, STOP_NONPHYSICAL = 3,
+             STOP_OUTPUT = 4 };
 
 constexpr double CFL_INIT = 1e9;     // timestep.cpp:8
 
@@ -943,12 +944,15 @@ k_cfl(DevParams P, StateView W, Ctrl* ctrl) {
 
 // Start of one time_advance iteration (maincycle.cpp:14-47). mode 0: plain
 // step (dt from CFL or dt_fixed); mode 1: with the TotalTime / output-time
-// clipping and stop conditions of time_advance.
+// clipping and stop conditions of time_advance; mode 2: as mode 1, and the
+// loop also ends after a step whose if_output is set, so that the host can
+// write that step's output.
 __global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, double total_time,
                               double out_freq) {
     if (c->stop) return;
     const double eps = 1e-12;
-    if (mode == 1 && fabs(total_time - c->time) <= eps) {
+    c->output = 0;
+    if (mode >= 1 && fabs(total_time - c->time) <= eps) {
         c->stop = 1;
         c->stop_reason = STOP_TOTAL_TIME;
         c->stop_in_pre = 1;
@@ -958,13 +962,17 @@ __global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, do
     double dt = dt_fixed;
     if (dt_fixed < 0.0) dt = cfl * __longlong_as_double((long long)c->dtmin_bits);
     c->dtmin_bits = pos_double_bits(CFL_INIT);
-    if (mode == 1) {
+    if (mode >= 1) {
         double t = c->time;
-        if (t >= c->out_next - eps) c->out_next += out_freq;
+        if (t >= c->out_next - eps) {
+            c->out_next += out_freq;
+            c->output = 1;
+        }
         if (t + dt > total_time) dt = total_time - t;
         if (t + dt > c->out_next) {
             dt = c->out_next - t;
             c->out_next += out_freq;
+            c->output = 1;
         }
         if (dt <= eps) {
             c->stop = 1;
@@ -989,9 +997,12 @@ __global__ void k_control_post(Ctrl* c, int mode, double total_time, long long n
         c->stop_reason = STOP_NONPHYSICAL;
         return;
     }
-    if (mode == 1 && c->time >= total_time) {
+    if (mode >= 1 && c->time >= total_time) {
         c->stop = 1;
         c->stop_reason = STOP_TOTAL_TIME;
+    } else if (mode == 2 && c->output) {
+        c->stop = 1;
+        c->stop_reason = STOP_OUTPUT;
     }
 }
 

@@ -231,6 +231,27 @@ class Solver:
                                             ctypes.byref(k)))
         return t.value, k.value
 
+    def time_advance_segment(self, max_steps: int):
+        """time_advance ending early after an output step; returns
+        (current_time, steps_done, events) with events a set of "output", "end"."""
+        t = ctypes.c_double()
+        k = ctypes.c_int()
+        ev = ctypes.c_int()
+        self._ck(self.lib.ns3d_time_advance_segment(self.ctx, int(max_steps), ctypes.byref(t),
+                                                    ctypes.byref(k), ctypes.byref(ev)))
+        events = {n for b, n in ((1, "output"), (2, "end")) if ev.value & b}
+        return t.value, k.value, events
+
+    def run(self, workdir: str = ".", max_steps: int | None = None, verbose: bool = True):
+        """time_advance with the reference's monitor and output files under
+        ``workdir``/output (maincycle.cpp:7-112). Returns (current_time, steps)."""
+        t = ctypes.c_double()
+        k = ctypes.c_int()
+        n = self.params.max_steps if max_steps is None else int(max_steps)
+        self._ck(self.lib.ns3d_run(self.ctx, workdir.encode(), n, int(bool(verbose)),
+                                   ctypes.byref(t), ctypes.byref(k)))
+        return t.value, k.value
+
     def step(self, nsteps: int = 1) -> None:
         self._ck(self.lib.ns3d_step(self.ctx, int(nsteps)))
 
@@ -313,9 +334,16 @@ class Solver:
         self._ck(self.lib.ns3d_energy_spectrum(self.ctx, _dptr(out), int(nbins)))
         return out
 
-    def compute_turbulence_statistics(self) -> dict:
+    def compute_turbulence_statistics(self, spectrum=None) -> dict:
+        """The statistics row; from `spectrum` (E(k), k = 0..) when given, else
+        from the state's own spectrum at full precision."""
         s = TurbStats()
-        self._ck(self.lib.ns3d_turbulence_stats(self.ctx, ctypes.byref(s)))
+        if spectrum is None:
+            self._ck(self.lib.ns3d_turbulence_stats(self.ctx, ctypes.byref(s)))
+        else:
+            e = np.ascontiguousarray(spectrum, dtype=np.float64)
+            self._ck(self.lib.ns3d_turbulence_stats_spectrum(self.ctx, _dptr(e), len(e),
+                                                             ctypes.byref(s)))
         return {n: getattr(s, n) for n, _ in TurbStats._fields_}
 
     def residuals(self) -> np.ndarray:
