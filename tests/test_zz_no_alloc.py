@@ -1,7 +1,11 @@
 """ns3d_compute_rhs_noalloc, the entry point for callers that may not allocate
 device memory (their GPU memory belongs to another allocator or budget): it
 must give the same RHS as the context-based ns3d_compute_rhs, call after call,
-while the test (not the entry point) owns every buffer it touches."""
+and match the oracle, while the test (not the entry point) owns every buffer
+it touches. Two boxes: 24x20x16 (the per-thread x sweep and the per-cell
+viscous kernel) and 64x32x32, the largest box the fixed scratch holds (65536
+cells), which takes the warp-per-row x sweep and the tiled viscous kernel
+(whose FP32 form reads the viscous fluxes inside the scratch as float4)."""
 import ctypes
 
 import numpy as np
@@ -9,11 +13,14 @@ import pytest
 
 import ns3d_cpp_b200 as ns
 from ns3d_cpp_b200 import _lib, initial
-from conftest import relerr
+from conftest import ref_cfg, relerr
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12  # both sides run the same kernels; the parity tests' FP64 bound
+# against the FP64 oracle: the FP64 form's parity bound, the FP32 form's RHS bound
+TOL_ORACLE = {"fp64": 1e-12, "fp32acc64": 5e-5}
+BOXES = [(16, 20, 24), (32, 32, 64)]  # (nz, ny, nx)
 
 
 def params(precision, nz=16, ny=20, nx=24):
@@ -30,11 +37,21 @@ def box_input(p, seed):
     return np.ascontiguousarray(W[:, :p.global_nz, :p.global_ny, :p.global_nx])
 
 
+def oracle_cfg(p):
+    cfg = ref_cfg(p.global_nx)
+    cfg.update(global_ny=p.global_ny, global_nz=p.global_nz)
+    return cfg
+
+
+@pytest.mark.parametrize("box", BOXES, ids=lambda b: "x".join(map(str, b[::-1])))
 @pytest.mark.parametrize("precision", ["fp64", "fp32acc64"])
-def test_noalloc_rhs_matches_compute_rhs_two_calls(precision):
+def test_noalloc_rhs_matches_compute_rhs_two_calls(oracle_mod, precision, box):
     import torch
     lib = _lib.load()
-    p = params(precision)
+    nz, ny, nx = box
+    p = params(precision, nz=nz, ny=ny, nx=nx)
+    assert nx * ny * nz <= 65536
+    orc = oracle_mod.Oracle(oracle_cfg(p))
     stream = torch.cuda.current_stream().cuda_stream
     for seed in (1, 2):  # two calls in a row, different inputs
         W = box_input(p, seed)
@@ -50,6 +67,8 @@ def test_noalloc_rhs_matches_compute_rhs_two_calls(precision):
         assert st == 0
         got = d_out.cpu().numpy()
         assert np.all(relerr(got, want) <= TOL), relerr(got, want)
+        ref = orc.rhs(W)
+        assert np.all(relerr(got, ref) <= TOL_ORACLE[precision]), relerr(got, ref)
 
 
 def test_noalloc_rejects_boxes_above_its_scratch():
