@@ -98,29 +98,75 @@ def dist_barrier(dist, use_cuda: bool):
 # ----------------------------------------------------------------------------
 
 class ClockSampler:
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    polled from a thread every 5 ms (so even a 0.1 s region gets ~20
+    samples), or nvidia-smi -lms 20 where NVML is unavailable."""
+    PERIOD_S = 0.005
+    NAMES = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+             ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
+        self.rows = []          # (sm_mhz, max_mhz, reason bits)
+        self.source = None
+        self._stop = None
+        self._thread = None
         self.proc = None
         self.path = None
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
     def __enter__(self):
+        import threading
+        try:
+            import pynvml
+            h = self._nvml_handle()
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self._stop = threading.Event()
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((float(sm), float(mx), int(rs)))
+                    except Exception:
+                        pass
+                    self._stop.wait(self.PERIOD_S)
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+            self.source = "nvml 5 ms"
+            return self
+        except Exception:
+            self._thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.fh,
                 stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi 20 ms"
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -128,31 +174,24 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
             self.fh.close()
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                        bits = sum(b for (_, b), v in zip(self.NAMES, parts[5:9])
+                                   if v.lower() == "active")
+                        mx = float(parts[2]) if parts[2].replace(".", "").isdigit() else 0.0
+                        self.rows.append((float(parts[1]), mx, bits))
+            os.unlink(self.path)
 
     def summary(self):
-        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        if not self.path or not os.path.exists(self.path):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows),
+               "source": self.source}
+        if not self.rows:
             return out
-        rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
-            return out
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in rows:
-            for k, name in enumerate(names):
-                if r[5 + k].lower() == "active":
-                    reasons.add(name)
-        out.update(sm_mhz=statistics.median(sm) if sm else None,
-                   sm_max_mhz=max(mx) if mx else None, reasons=sorted(reasons),
-                   samples=len(rows))
+        reasons = sorted({name for _, _, bits in self.rows for name, b in self.NAMES if bits & b})
+        out.update(sm_mhz=statistics.median(r[0] for r in self.rows),
+                   sm_max_mhz=max(r[1] for r in self.rows), reasons=reasons)
         return out
 
 
@@ -195,10 +234,12 @@ def kernel_bytes_per_cell(cls: str, rsize: int) -> float:
     fv = 12 if rsize == 4 else 9
     if cls == "visc_flux":
         return 4 * 8 + fv * rsize
-    if cls == "update":
+    if cls in ("update", "sweep_z_update"):
         # current + recorded state (stage 1 reads only the recorded one: the
         # mean over the three stages is 5/3 state reads), T_acc, the viscous
-        # flux values, 6 doubles written
+        # flux values, 6 doubles written; the fused z sweep reads the current
+        # state for its splits and the same cell's values again for the stage
+        # (cache hits), so the same bytes
         return (5.0 / 3.0) * w + 5 * rsize + fv * rsize + 6 * 8
     return 0.0
 
@@ -288,7 +329,7 @@ def e2e_run(torch, ns, n, W, steps, device):
             "path": "Solver.upload_primitive(pinned host) + step(1) + compute_total_energy"}
 
 
-def adjoint_cost(torch, ns, device, nsteps=200, K=20, n=64):
+def adjoint_cost(torch, ns, device, nsteps=200, K=20, n=64, fd_dirs=2):
     """Adjoint workload: Taylor-Green 64^3 + seeded 1e-3 solenoidal perturbation,
     Re 400, Ma 0.2, SW (entropy fix 1e-3) + WENO5, C8th, 200 RK3 steps,
     checkpoint every 20. Cost = (checkpointed forward + reverse sweep with
@@ -319,24 +360,74 @@ def adjoint_cost(torch, ns, device, nsteps=200, K=20, n=64):
             e1.synchronize()
             return e0.elapsed_time(e1) / 1e3, time.perf_counter() - t0, out
         fwd_dev, fwd_wall, _ = timed(lambda: s.step(nsteps))
-        adj_dev, adj_wall, (grad, J, _) = timed(lambda: s.adjoint(nsteps, K))
+        adj_dev, adj_wall, (grad, J, dts) = timed(lambda: s.adjoint(nsteps, K))
+
+        # accuracy, measured here: the gradient along random solenoidal
+        # directions against the 4-point central difference of the forward
+        # with the recorded dt sequence (h = 1e-6 per unit-rms direction)
+        def J_of(Wx):
+            s.upload_primitive(Wx)
+            s.step_dts(dts)
+            return s.compute_total_energy()
+        h = 1e-6
+        gnorm = math.sqrt(float(np.sum(grad[1:4] ** 2)))
+        fd = []
+        for k in range(fd_dirs):
+            d = np.zeros_like(W)
+            d[1:4] = initial.solenoidal_field(n, k0=4.0, seed=100 + k)
+            d[1:4] /= math.sqrt(float(np.mean(d[1:4] ** 2)))
+            Jd = (-J_of(W + 2 * h * d) + 8 * J_of(W + h * d) - 8 * J_of(W - h * d)
+                  + J_of(W - 2 * h * d)) / (12 * h)
+            ad = float(np.sum(grad[1:4] * d[1:4]))
+            fd.append({"rel": abs(Jd - ad) / abs(ad),
+                       "rel_to_norm": abs(Jd - ad) / (gnorm * math.sqrt(float(np.sum(d[1:4] ** 2))))})
+        J_replay = J_of(W)
     return {"workload": f"Taylor-Green {n}^3 + 1e-3 solenoidal perturbation, Re 400, Ma 0.2, "
                         f"SW(eps 1e-3)+WENO5, C8th, {nsteps} RK3 steps, checkpoint every {K}",
             "forward_s": fwd_dev, "adjoint_s": adj_dev, "ratio": adj_dev / fwd_dev,
             "ratio_wall": adj_wall / fwd_wall, "J": J,
-            "accuracy": "vs FP64 autograd reference 1e-9 (norm); vs 4-point central FD on 16 "
-                        "random directions: median 1.9e-7 relative, all <= 1e-7 of |J'||d| "
-                        "(tests/test_adjoint.py)"}
+            "J_replay_rel": abs(J_replay - J) / abs(J),
+            "fd_directions": fd,
+            "fd": "4-point central difference at h = 1e-6 per unit-rms solenoidal direction "
+                  "(k0 4, seeds 100..), forward replayed with the adjoint's dt sequence"}
 
 
 def ncu_traffic():
-    """DRAM bytes per launch per kernel class from the committed ncu summary."""
+    """DRAM bytes per cell per kernel class, from the ncu capture recorded in
+    profiles/ncu_traffic.json (dram__bytes_read.sum + dram__bytes_write.sum of
+    one launch of each class, on a smaller box; `cells` names its size)."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
             return json.load(f)
     except Exception:
         return {}
+
+
+def oracle_rhs_errors(ns, n, W, device):
+    """The GPU's RHS of the benchmark field in both forms against the FP64
+    oracle's (the C restatement, bit-exact against the reference), max|a-b| /
+    max|b| per conserved variable. Part of the CPU leg: the oracle runs on the
+    host's cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    w = WORKLOAD
+    two_pi = "6.283185307179586"
+    cfg = dict(gamma=w["gamma"], Pr=w["Pr"], Ma=w["Ma"], Re=w["Re"], cfl=w["cfl"], dt_fixed=-1,
+               fvs_type="StagerWarming", recon="WENO5", vis_scheme="C8th",
+               global_nx=n, global_ny=n, global_nz=n, Lx=two_pi, Ly=two_pi, Lz=two_pi,
+               char_recon="true" if w.get("char") else "false")
+    t0 = time.perf_counter()
+    ref = oracle.Oracle(cfg).rhs(W)
+    t_orc = time.perf_counter() - t0
+    den = np.max(np.abs(ref), axis=(1, 2, 3))
+    out = {"oracle_s": t_orc, "threads": os.environ.get("OMP_NUM_THREADS", str(os.cpu_count()))}
+    for prec in ("fp64", "fp32acc64"):
+        with ns.Solver(make_params(ns, n, prec), device=device) as s:
+            s.upload_primitive(W)
+            r = s.compute_rhs()
+        out[prec] = float(np.max(np.max(np.abs(r - ref), axis=(1, 2, 3)) / den))
+    return out
 
 
 def our_arm(args, rank, world, local):
@@ -351,6 +442,21 @@ def our_arm(args, rank, world, local):
     W = workload_input(n)
     ncell = n ** 3
     peak, peak_kind = measured_peaks()
+
+    if args.only_fp64:
+        # diagnostic mode (kernel captures of the FP64 form): its steps alone
+        with ns.Solver(make_params(ns, n, "fp64"), device=local) as s:
+            s.upload_primitive(W)
+            ms64, _, prof64 = timed_steps(torch, s, args.steps, args.warmup, dist, use_cuda)
+        ms64 = dist_max(dist, ms64, use_cuda)
+        if rank == 0:
+            print(json.dumps({"form": "fp64", "n": n, "steps": args.steps,
+                              "steps_per_s": world * args.steps / (ms64 / 1e3),
+                              "kernels_ms_per_launch": {c: (v[0] / v[1] if v[1] else None)
+                                                        for c, v in prof64.items()}}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # --- the headline form: FP32 stencils, FP64 accumulation ---
     with ns.Solver(make_params(ns, n, "fp32acc64"), device=local) as s:
@@ -392,19 +498,20 @@ def our_arm(args, rank, world, local):
                          "achieved_gbs": b / (kms / cnt / 1e3) / 1e9 if b else None}
     dom = max((c for c in kern if c != "other"), key=lambda c: kern[c]["ms_total"])
     tr = ncu_traffic()
-    # captured traffic belongs to the component-wise kernels
-    traffic = None if WORKLOAD.get("char") else tr.get(f"fp32acc64/{dom}")
-    traffic = None if traffic is None else traffic * 1e9 * (ncell / 256 ** 3)
-    # algorithmic bytes of the captured launch (the update capture is a stage-2 launch)
-    cap_alg = tr.get(f"fp32acc64/{dom}/alg_bytes_per_cell")
-    traffic_alg = None if traffic is None else (cap_alg or kernel_bytes_per_cell(dom, rsize)) * ncell
+    # captured traffic belongs to the component-wise kernels: bytes per cell of
+    # the captured launch, times this run's cells
+    cap = None if WORKLOAD.get("char") else (tr.get("fp32acc64") or {}).get(dom)
+    traffic = None if cap is None else cap["dram_bytes_per_cell"] * ncell
     ach = kern[dom]["achieved_gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
                 "alg_bytes_per_cell": kernel_bytes_per_cell(dom, rsize),
                 "alg_bytes_per_launch": kern[dom]["alg_bytes_per_launch"],
-                "traffic_source": tr.get("source") if traffic is not None else None,
-                "traffic_alg_bytes": traffic_alg}
+                "traffic_capture": None if cap is None else {
+                    "metric": "dram__bytes_read.sum + dram__bytes_write.sum, one launch",
+                    "cells": tr.get("cells"), "stage": cap.get("stage"),
+                    "scaled": f"per cell of the captured box, times {ncell} cells",
+                    "alg_bytes_per_cell_of_capture": cap.get("alg_bytes_per_cell")}}
     step_ach = STEP_BYTES_PER_CELL * ncell * (value / world) / 1e9
     roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s",
                      "frac": step_ach / peak, "alg_bytes_per_cell_step": STEP_BYTES_PER_CELL}
@@ -412,6 +519,11 @@ def our_arm(args, rank, world, local):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample_steps, n)
+        try:
+            cpu["oracle_rhs_errors"] = oracle_rhs_errors(ns, n, W, local)
+        except Exception as e:  # reported, never fatal for the GPU line
+            cpu["oracle_rhs_errors"] = {"error": str(e)}
+    orc = (cpu or {}).get("oracle_rhs_errors") or {}
 
     line = {
         "metric": METRIC,
@@ -424,12 +536,19 @@ def our_arm(args, rank, world, local):
                    "l2": f"inputs larger than L2: {6 * ncell * 8 / 1e6:.0f} MB per state buffer",
                    "parallelism": f"replicas x{world}"},
         "gcell_per_s": value * ncell / 1e9,
+        "fp64_steps_per_s": fp64_sps,
+        "fp32_over_fp64": None if fp64_sps is None else value / fp64_sps,
+        "ke_err_fp32_vs_fp64": None if errors is None else errors["kinetic_energy"],
+        "dissipation_err_fp32_vs_fp64": None if errors is None else errors["dissipation"],
+        "spectrum_err_fp32_vs_fp64": None if errors is None else errors["spectrum_max"],
+        "rhs_err_fp32_vs_oracle": orc.get("fp32acc64"),
+        "rhs_err_fp64_vs_oracle": orc.get("fp64"),
+        "adjoint_over_forward_cost": None if adjoint is None else adjoint["ratio"],
         "fp64": None if fp64_sps is None else {
             "steps_per_s": fp64_sps, "gcell_per_s": fp64_sps * ncell / 1e9,
             "steps": k64, "ms_per_step": ms64_max / k64,
             "kernels_ms_per_launch": {c: (v[0] / v[1] if v[1] else None)
                                       for c, v in prof64.items()}},
-        "fp32_over_fp64": None if fp64_sps is None else value / fp64_sps,
         "errors_fp32_vs_fp64": errors,
         "adjoint_over_forward": adjoint,
         "roofline": roofline, "roofline_step": roofline_step, "kernels": kern,
@@ -504,6 +623,22 @@ def run_cpu(steps: int, warm: int, n_equiv: int):
                        f"steps/s scaled to {n_equiv}^3 by cell count; wall {wall:.1f} s")}
 
 
+def run_direct(n: int, steps: int = 1):
+    """One single-rank replica of the reference on the benchmark's own box
+    (n^3, one host core): the figure the 64^3 replicas are scaled to n^3
+    from. Returns seconds per step."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    kind = "reference" if oracle.have_ref() else "port"
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(1) as pool:
+        s_step = pool.map(_cpu_worker, [(kind, n, steps, 0, bool(WORKLOAD.get("char")))])[0]
+    return {"n": n, "steps": steps, "s_per_step_one_core": s_step, "kind": kind,
+            "wall_s": time.perf_counter() - t0}
+
+
 def cpu_baseline(steps: int, n: int):
     try:
         return run_cpu(steps, 0, n)
@@ -515,6 +650,17 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     res = run_cpu(args.steps, args.warmup, args.n)
+    direct = None
+    if getattr(args, "direct_steps", 1) > 0:
+        try:
+            direct = run_direct(args.n, getattr(args, "direct_steps", 1))
+            per_cell_direct = direct["s_per_step_one_core"] / args.n ** 3
+            per_cell_replica = res["s_per_step_one_core"] / CPU_SAMPLE_N ** 3
+            # 1.0: scaling the replicas' rate to n^3 by cell count holds
+            direct["per_cell_vs_replica"] = per_cell_direct / per_cell_replica
+            direct["steps_per_s_one_core"] = 1.0 / direct["s_per_step_one_core"]
+        except Exception as e:  # reported, never fatal for the line
+            direct = {"error": str(e)}
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": "steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -524,22 +670,27 @@ def reference_arm(args, rank, world):
                              "kind": res["kind"], "sample": res["sample"]},
             "e2e": {"value": res["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "cell_updates_per_s": res["cell_updates_per_s"]}
+            "cell_updates_per_s": res["cell_updates_per_s"],
+            "direct_full_size": direct}
     print(json.dumps(line), flush=True)
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--err-steps", type=int, default=500)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--direct-steps", type=int, default=1,
+                    help="reference arm: steps of one single-core replica at the full size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true", help="only the headline form")
+    ap.add_argument("--only-fp64", action="store_true",
+                    help="diagnostic: time the plain FP64 form alone (for kernel captures)")
     ap.add_argument("--skip-adjoint", action="store_true", help="no adjoint cost measurement")
     ap.add_argument("--char-recon", action="store_true",
                     help="characteristic-wise reconstruction in both arms (char_recon)")

@@ -247,7 +247,9 @@ ns3d_status ns3d_compute_rhs_noalloc(const ns3d_params *p, const double *rho, co
 enum {
     NS3D_KERNEL_SWEEP_X = 0, NS3D_KERNEL_SWEEP_Y = 1, NS3D_KERNEL_SWEEP_Z = 2,
     NS3D_KERNEL_VISC_FLUX = 3, NS3D_KERNEL_UPDATE = 4, NS3D_KERNEL_OTHER = 5,
-    NS3D_KERNEL_CLASSES = 6
+    /* the z sweep fused with the stage update (component-wise schemes) */
+    NS3D_KERNEL_SWEEP_Z_UPDATE = 6,
+    NS3D_KERNEL_CLASSES = 7
 };
 /* The cudaStream_t every kernel of this context is launched on. */
 ns3d_status ns3d_get_stream(ns3d_ctx *ctx, void **stream);
@@ -297,13 +299,21 @@ ns3d_status ns3d_read_tecplot(ns3d_ctx *ctx, const char *path);
 
 /* Binary checkpoint of the context (no counterpart in the reference, which restarts
  * from its 9-digit Tecplot field, initialization.cpp:35-100): the current state's
- * rho, u, v, w, p, T bit for bit, the clock of ns3d_time_advance and the state's CFL
- * minimum, with a 64-bit checksum. Reading it into a context of the same grid gives a
- * run that repeats the uninterrupted one exactly (U0 recorded from the read state).
- * NS3D_ERR_FILE: unreadable, not a checkpoint, truncated or checksum mismatch;
- * NS3D_ERR_INVALID: another grid. */
+ * rho, u, v, w, p, T bit for bit, the clock and step count of ns3d_time_advance, the
+ * state's CFL minimum and the gas it belongs to, with a 64-bit checksum. Reading it
+ * into a context of the same grid and gas gives a run that repeats the uninterrupted
+ * one exactly (U0 recorded from the read state; ns3d_run numbers on from the stored
+ * step count). NS3D_ERR_FILE: unreadable, not a (version 2) checkpoint, truncated or
+ * checksum mismatch; NS3D_ERR_INVALID: another grid or another gas (gamma, Rgas, mu,
+ * Pr, Cp or Sutherland's S/Tref: T = p/(rho Rgas) and the CFL minimum would no longer
+ * belong to the context). ns3d_checkpoint_check tests a file's header against
+ * parameters on the host, without a context or a GPU. */
 ns3d_status ns3d_checkpoint_write(ns3d_ctx *ctx, const char *path);
 ns3d_status ns3d_checkpoint_read(ns3d_ctx *ctx, const char *path);
+ns3d_status ns3d_checkpoint_check(const char *path, const ns3d_params *p);
+/* Steps the time_advance loops of this context have completed (the step number
+ * beside ns3d_time_advance's clock; restored by ns3d_checkpoint_read). */
+ns3d_status ns3d_completed_steps(ns3d_ctx *ctx, long long *steps);
 
 /* compute_diagnostics (postprocess.cpp:7-98) after a step: res[q] = sqrt(sum (U - U0)^2
  * dx^3) / max |U| for rho, rhou, rhov, rhow, E, with U the current state and U0 the
@@ -345,8 +355,11 @@ ns3d_status ns3d_stats_write(const char *path, double time, const ns3d_turb_stat
  * post-processing (spectrum file + statistics row); after every output step, the
  * Tecplot field time_<100000 t>/field_rank0.dat (post_basicfield) and the isotropic
  * post-processing. verbose: the reference's "[Step n] ..." monitor lines on stdout.
- * Steps are numbered from 1 in each call. Between monitor and output steps the loop
- * runs on the device without host synchronisation. NS3D_ERR_INVALID for
+ * Steps are numbered on from the context's completed steps (ns3d_completed_steps: 0
+ * for a new context, the stored count after ns3d_checkpoint_read), and `max_steps` is
+ * the last step number, as in the reference's loop; a run continued from a checkpoint
+ * so writes the files of the uninterrupted run. Between monitor and output steps the
+ * loop runs on the device without host synchronisation. NS3D_ERR_INVALID for
  * monitor_Stepfreq <= 0 (a division by zero in the reference). */
 ns3d_status ns3d_run(ns3d_ctx *ctx, const char *workdir, int max_steps, int verbose,
                      double *time, int *steps_done);

@@ -65,6 +65,8 @@ _SIGS = {
     "ns3d_run": (_i, [_vp, ctypes.c_char_p, _i, _i, _D, ctypes.POINTER(ctypes.c_int)]),
     "ns3d_checkpoint_write": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_checkpoint_read": (_i, [_vp, ctypes.c_char_p]),
+    "ns3d_checkpoint_check": (_i, [ctypes.c_char_p, _vp]),
+    "ns3d_completed_steps": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "ns3d_residuals_write": (_i, [ctypes.c_char_p, _i, _D, ctypes.c_double]),
     "ns3d_read_tecplot": (_i, [_vp, ctypes.c_char_p]),
     "ns3d_get_stream": (_i, [_vp, _pvp]),

@@ -34,6 +34,10 @@ extern template cudaError_t launch_visc_flux<float>(const LaunchCfg&, StateView,
 extern template cudaError_t launch_update<float>(const LaunchCfg&, int, StateView, StateView,
                                                  const float*, const float*, StateOut, Ctrl*);
 extern template cudaError_t launch_rhs_out<float>(const LaunchCfg&, const float*, const float*, double*);
+extern template cudaError_t launch_sweep_z_update<double>(const LaunchCfg&, int, StateView, StateView,
+                                                          const double*, const double*, StateOut, Ctrl*);
+extern template cudaError_t launch_sweep_z_update<float>(const LaunchCfg&, int, StateView, StateView,
+                                                         const float*, const float*, StateOut, Ctrl*);
 }  // namespace ns3d
 
 struct ns3d_ctx {
@@ -60,12 +64,14 @@ struct ns3d_ctx {
     int sums_blocks = 0;
     bool dtmin_valid = false;
     double time = 0.0, out_next = 0.0;
+    long long steps = 0;         // completed steps (the time_advance step count beside `time`)
     int last_events = 0;         // NS3D_EVENT_* of the last stepping call
     // spectrum
     cufftHandle fft = 0;
     bool fft_ready = false;
     cufftDoubleComplex* spec = nullptr;
     double* bins = nullptr;
+    double* spec_part = nullptr;  // per-block bin partials of the spectrum
     // instrumentation
     long long launches = 0;
     bool prof_on = false;
@@ -339,33 +345,89 @@ __global__ void k_prim2cons(DevParams P, StateView W, double* __restrict__ U, do
     if (c) c[id] = sqrt(P.gamma * W.p[id] / Uc[0]);
 }
 
-// Shell binning of |u_hat|^2 (EnergySpectrum.cpp:99-125) from a D2Z transform
-// (x half-spectrum): modes strictly inside the half-space count twice.
-__global__ void k_spectrum_bin(const cufftDoubleComplex* __restrict__ X, int nx, int ny, int nz,
-                               double scale, int nbins, double* __restrict__ bins) {
-    extern __shared__ double sb[];
-    for (int b = threadIdx.x; b < nbins; b += blockDim.x) sb[b] = 0.0;
+// Shell binning of one velocity component's half spectrum (cuFFT D2Z of the
+// component, EnergySpectrum.cpp:108-125: E(k) += 0.5 |u_hat|^2 with
+// u_hat = X / N and k = floor(|k|); modes strictly inside the x half-space
+// stand for their conjugates and count twice), in a fixed order so that E(k)
+// is the same to the last bit on every call.
+//
+// A warp takes whole x rows (fixed (j, k), ic = 0 .. nx/2) of the half
+// spectrum in a fixed assignment. Along a row the shell index is
+// non-decreasing in ic, so the 32 values of a chunk fall into contiguous runs
+// of equal shell: a segmented shuffle reduction leaves each run's sum in its
+// first lane, which adds it to the warp's own shared bin array (no two lanes
+// write one bin in the same step). The block then sums its warps' arrays in
+// warp order into part[block][bin].
+constexpr int SPEC_WARPS = 4;
+constexpr int SPEC_BLOCKS = 4 * 148;
+
+// Shells a half spectrum can reach: floor(|k|) <= floor(sqrt((nx/2)^2 +
+// (ny/2)^2 + (nz/2)^2)); one more for safety, at most the reference's 2 nx + 1.
+inline int spectrum_bins_used(int nx, int ny, int nz) {
+    const double k2 = (double)(nx / 2) * (nx / 2) + (double)(ny / 2) * (ny / 2) +
+                      (double)(nz / 2) * (nz / 2);
+    const int nb = (int)std::sqrt(k2) + 2;
+    return nb < 2 * nx + 1 ? nb : 2 * nx + 1;
+}
+
+__global__ void __launch_bounds__(32 * SPEC_WARPS)
+k_spectrum_part(const cufftDoubleComplex* __restrict__ X, int nx, int ny, int nz, double scale,
+                int nbu, double* __restrict__ part) {
+    extern __shared__ double sb[];  // [SPEC_WARPS][nbu]
+    for (int b = threadIdx.x; b < SPEC_WARPS * nbu; b += blockDim.x) sb[b] = 0.0;
     __syncthreads();
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    double* wb = sb + wq * nbu;
     const int nxh = nx / 2 + 1;
-    const long long total = (long long)nxh * ny * nz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int ic = (int)(t % nxh);
-        const long long r = t / nxh;
+    const long long rows = (long long)ny * nz;
+    const long long warps = (long long)gridDim.x * SPEC_WARPS;
+    for (long long r = (long long)blockIdx.x * SPEC_WARPS + wq; r < rows; r += warps) {
         const int j = (int)(r % ny), k = (int)(r / ny);
-        const int k1 = ic;
         const int k2 = j <= ny / 2 ? j : j - ny;
         const int k3 = k <= nz / 2 ? k : k - nz;
-        const int kk = (int)sqrt(1.0 * (k1 * k1 + k2 * k2 + k3 * k3));
-        const double re = X[t].x * scale, im = X[t].y * scale;
-        double e = 0.5 * (re * re + im * im);
-        const bool self_conj = (ic == 0) || ((nx % 2 == 0) && ic == nx / 2);
-        if (!self_conj) e *= 2.0;
-        if (kk < nbins) atomicAdd(&sb[kk], e);
+        const int kt = k2 * k2 + k3 * k3;
+        for (int c0 = 0; c0 < nxh; c0 += 32) {
+            const int ic = c0 + lane;
+            double e = 0.0;
+            int kk = -1;
+            if (ic < nxh) {
+                const cufftDoubleComplex z = X[r * nxh + ic];
+                const double re = z.x * scale, im = z.y * scale;
+                e = 0.5 * (re * re + im * im);
+                const bool self_conj = (ic == 0) || ((nx % 2 == 0) && ic == nx / 2);
+                if (!self_conj) e *= 2.0;
+                kk = (int)sqrt(1.0 * (ic * ic + kt));
+            }
+            // segmented sum over runs of equal kk (contiguous: kk non-decreasing in ic)
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const double ev = __shfl_down_sync(0xffffffffu, e, off);
+                const int kv = __shfl_down_sync(0xffffffffu, kk, off);
+                if (lane + off < 32 && kv == kk) e += ev;
+            }
+            const int kprev = __shfl_up_sync(0xffffffffu, kk, 1);
+            const bool head = kk >= 0 && (lane == 0 || kprev != kk);
+            if (head && kk < nbu) wb[kk] += e;
+            __syncwarp();
+        }
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
-        if (sb[b] != 0.0) atomicAdd(&bins[b], sb[b]);
+    for (int b = threadIdx.x; b < nbu; b += blockDim.x) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < SPEC_WARPS; ++w) x += sb[w * nbu + b];
+        part[(long long)blockIdx.x * nbu + b] = x;
+    }
+}
+
+// bins[b] += sum over blocks of part[.][b], blocks in order.
+__global__ void k_spectrum_final(const double* __restrict__ part, int nblocks, int nbu,
+                                 double* __restrict__ bins) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbu) return;
+    double x = 0.0;
+    for (int k = 0; k < nblocks; ++k) x += part[(long long)k * nbu + b];
+    bins[b] += x;
 }
 
 ns3d_status validate(const ns3d_params* p, std::string& msg) {
@@ -427,9 +489,11 @@ ns3d_status read_ctrl(ns3d_ctx* ctx) {
     return NS3D_OK;
 }
 
-// The RHS pieces of the current state (sweeps + viscous flux) into tacc/fv.
+// The RHS pieces of the current state into tacc/fv: the sweeps along x, y and
+// (unless `dirs` is 2, when the z sweep is left to the fused stage kernel) z,
+// and the viscous flux.
 template <class R>
-ns3d_status rhs_parts_t(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl) {
+ns3d_status rhs_parts_t(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl, int dirs = 3) {
     R* tacc = (R*)ctx->tacc;
     if (ctx->overlap) {
         // the viscous flux (state -> fv) beside the sweeps (state -> T_acc):
@@ -444,12 +508,12 @@ ns3d_status rhs_parts_t(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl) {
         });
         if (s != NS3D_OK) return s;
         NS3D_CK(cudaEventRecord(ctx->ev_join, ctx->side));
-        for (int dir = 0; dir < 3; ++dir)
+        for (int dir = 0; dir < dirs; ++dir)
             NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X + dir, 1, launch_sweep<R>(ctx->L, dir, W, tacc, ctrl));
         NS3D_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
         return NS3D_OK;
     }
-    for (int dir = 0; dir < 3; ++dir)
+    for (int dir = 0; dir < dirs; ++dir)
         NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X + dir, 1, launch_sweep<R>(ctx->L, dir, W, tacc, ctrl));
     NS3D_LAUNCH(NS3D_KERNEL_VISC_FLUX, 1, launch_visc_flux<R>(ctx->L, W, (R*)ctx->fv, ctrl));
     return NS3D_OK;
@@ -461,11 +525,25 @@ ns3d_status launch_rhs_parts(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl) {
                                               : rhs_parts_t<float>(ctx, W, ctrl);
 }
 
+// One Shu-Osher stage Wc -> Wn (recorded state W0). Component-wise schemes:
+// x and y sweeps, the viscous flux, then the z sweep fused with the update
+// (k_sweep_ring<2, ..., FUSE>); characteristic-wise reconstruction: the three
+// sweeps, the viscous flux and k_update. Both give the same bits.
 template <class R>
-ns3d_status update_t(ns3d_ctx* ctx, int stage, StateView Wc, StateView W0, int bn) {
-    NS3D_LAUNCH(NS3D_KERNEL_UPDATE, 1,
-                launch_update<R>(ctx->L, stage, Wc, W0, (const R*)ctx->tacc, (const R*)ctx->fv,
-                                 outv(ctx, bn), ctx->ctrl));
+ns3d_status stage_t(ns3d_ctx* ctx, int stage, StateView Wc, StateView W0, StateOut Wn) {
+    const R* tacc = (const R*)ctx->tacc;
+    const R* fv = (const R*)ctx->fv;
+    if (ctx->L.chr) {
+        ns3d_status s = rhs_parts_t<R>(ctx, Wc, ctx->ctrl);
+        if (s != NS3D_OK) return s;
+        NS3D_LAUNCH(NS3D_KERNEL_UPDATE, 1,
+                    launch_update<R>(ctx->L, stage, Wc, W0, tacc, fv, Wn, ctx->ctrl));
+        return NS3D_OK;
+    }
+    ns3d_status s = rhs_parts_t<R>(ctx, Wc, ctx->ctrl, 2);
+    if (s != NS3D_OK) return s;
+    NS3D_LAUNCH(NS3D_KERNEL_SWEEP_Z_UPDATE, 1,
+                launch_sweep_z_update<R>(ctx->L, stage, Wc, W0, tacc, fv, Wn, ctx->ctrl));
     return NS3D_OK;
 }
 
@@ -478,21 +556,14 @@ StateOut out_at(double* base, long long n) {
 }
 
 ns3d_status stage_at(ns3d_ctx* ctx, int stage, double* wc, double* w0, double* wn) {
-    const StateView Wc = view_at(wc, ctx->n), W0 = view_at(w0, ctx->n);
-    ns3d_status s = launch_rhs_parts(ctx, Wc, ctx->ctrl);
-    if (s != NS3D_OK) return s;
-    NS3D_LAUNCH(NS3D_KERNEL_UPDATE, 1,
-                launch_update<double>(ctx->L, stage, Wc, W0, (const double*)ctx->tacc,
-                                      (const double*)ctx->fv, out_at(wn, ctx->n), ctx->ctrl));
-    return NS3D_OK;
+    return stage_t<double>(ctx, stage, view_at(wc, ctx->n), view_at(w0, ctx->n),
+                           out_at(wn, ctx->n));
 }
 
 ns3d_status launch_stage(ns3d_ctx* ctx, int stage, int bc, int b0, int bn) {
     const StateView Wc = view(ctx, bc), W0 = view(ctx, b0);
-    ns3d_status s = launch_rhs_parts(ctx, Wc, ctx->ctrl);
-    if (s != NS3D_OK) return s;
-    return ctx->p.precision == NS3D_PREC_FP64 ? update_t<double>(ctx, stage, Wc, W0, bn)
-                                              : update_t<float>(ctx, stage, Wc, W0, bn);
+    return ctx->p.precision == NS3D_PREC_FP64 ? stage_t<double>(ctx, stage, Wc, W0, outv(ctx, bn))
+                                              : stage_t<float>(ctx, stage, Wc, W0, outv(ctx, bn));
 }
 
 // One runge_kutta_3 on the device with dt from ctrl->dt. Buffer rotation keeps
@@ -757,6 +828,7 @@ ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
     if (ctx->fft_ready) cufftDestroy(ctx->fft);
     cudaFree(ctx->spec);
     cudaFree(ctx->bins);
+    cudaFree(ctx->spec_part);
     cudaFree(ctx->wmem);
     cudaFree(ctx->tacc);
     cudaFree(ctx->fv);
@@ -964,6 +1036,7 @@ static ns3d_status run_steps(ns3d_ctx* ctx, int mode, int nsteps, int* steps_don
     else if (d < nsteps && h.stop_in_pre) ctx->rec = ctx->cur;  // recorded, then stopped
     else ctx->rec = d > 0 ? (cur0 + d - 1) % 3 : rec0;
     if (steps_done) *steps_done = d;
+    ctx->steps += d;
     ctx->time = h.time;
     ctx->out_next = h.out_next;
     ctx->dtmin_valid = true;
@@ -1045,11 +1118,15 @@ struct CkptHeader {
     uint64_t dtmin_bits;         // the CFL minimum's bit pattern when dtmin_valid
     uint32_t dtmin_valid, reserved;
     double dx, dy, dz;
+    // the gas the state belongs to: T = p / (rho Rgas) is stored, and the CFL
+    // minimum carries the sound speed sqrt(gamma p / rho)
+    double gamma, Rgas, mu, Pr, Cp, sutherland_s;
+    int64_t steps;               // completed time_advance steps (ns3d_run numbers on from it)
     uint64_t payload_hash;       // hash_words over the six arrays
 };
-static_assert(sizeof(CkptHeader) == 96, "checkpoint header layout");
+static_assert(sizeof(CkptHeader) == 152, "checkpoint header layout");
 constexpr char kCkptMagic[8] = {'N', 'S', '3', 'D', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCkptVersion = 1;
+constexpr uint32_t kCkptVersion = 2;
 
 // FNV-1a over 64-bit words: chunks of 2^17 words hashed on the host's threads,
 // the chunk hashes folded in order, so the value does not depend on the
@@ -1098,6 +1175,13 @@ ns3d_status ns3d_checkpoint_write(ns3d_ctx* ctx, const char* path) {
     h.dx = ctx->p.dx;
     h.dy = ctx->p.dy;
     h.dz = ctx->p.dz;
+    h.gamma = ctx->p.gamma;
+    h.Rgas = ctx->p.Rgas;
+    h.mu = ctx->p.mu;
+    h.Pr = ctx->p.Pr;
+    h.Cp = ctx->p.Cp;
+    h.sutherland_s = ctx->p.sutherland_s_over_tref;
+    h.steps = ctx->steps;
     const long long nw = 6 * ctx->n;
     std::vector<double> buf((size_t)nw);
     if (ctx->dtmin_valid)
@@ -1115,22 +1199,63 @@ ns3d_status ns3d_checkpoint_write(ns3d_ctx* ctx, const char* path) {
     return ok ? NS3D_OK : fail(ctx, NS3D_ERR_FILE, std::string("write failed: ") + path);
 }
 
+namespace {
+
+// Opens `path` and checks its header against `p`; on NS3D_OK *f is positioned
+// at the payload.
+ns3d_status checkpoint_open(const char* path, const ns3d_params* p, CkptHeader* h, FILE** f,
+                            std::string* msg) {
+    *f = std::fopen(path, "rb");
+    if (!*f) {
+        *msg = std::string("cannot open ") + path;
+        return NS3D_ERR_FILE;
+    }
+    ns3d_status s = NS3D_OK;
+    if (std::fread(h, sizeof *h, 1, *f) != 1 || std::memcmp(h->magic, kCkptMagic, sizeof h->magic) ||
+        h->version != kCkptVersion || h->header_bytes != sizeof *h) {
+        *msg = std::string("not a version 2 checkpoint: ") + path;
+        s = NS3D_ERR_FILE;
+    } else if (h->nx != p->global_nx || h->ny != p->global_ny || h->nz != p->global_nz ||
+               !same_bits(h->dx, p->dx) || !same_bits(h->dy, p->dy) || !same_bits(h->dz, p->dz)) {
+        *msg = "the checkpoint's grid differs from the parameters'";
+        s = NS3D_ERR_INVALID;
+    } else if (!same_bits(h->gamma, p->gamma) || !same_bits(h->Rgas, p->Rgas) ||
+               !same_bits(h->mu, p->mu) || !same_bits(h->Pr, p->Pr) || !same_bits(h->Cp, p->Cp) ||
+               !same_bits(h->sutherland_s, p->sutherland_s_over_tref)) {
+        *msg = "the checkpoint's gas (gamma, Rgas, mu, Pr, Cp or Sutherland S) differs from the "
+               "parameters'";
+        s = NS3D_ERR_INVALID;
+    }
+    if (s != NS3D_OK) {
+        std::fclose(*f);
+        *f = nullptr;
+    }
+    return s;
+}
+
+}  // namespace
+
+ns3d_status ns3d_checkpoint_check(const char* path, const ns3d_params* p) {
+    if (!path || !p) return NS3D_ERR_INVALID;
+    ns3d_params q = *p;
+    ns3d_params_derive(&q);
+    CkptHeader h{};
+    FILE* f = nullptr;
+    std::string msg;
+    const ns3d_status s = checkpoint_open(path, &q, &h, &f, &msg);
+    if (f) std::fclose(f);
+    if (s != NS3D_OK) std::fprintf(stderr, "ns3d_checkpoint_check: %s\n", msg.c_str());
+    return s;
+}
+
 ns3d_status ns3d_checkpoint_read(ns3d_ctx* ctx, const char* path) {
     if (!ctx || !path) return NS3D_ERR_INVALID;
     NS3D_CK(cudaSetDevice(ctx->device));
-    FILE* f = std::fopen(path, "rb");
-    if (!f) return fail(ctx, NS3D_ERR_FILE, std::string("cannot open ") + path);
     CkptHeader h{};
-    if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, kCkptMagic, sizeof h.magic) ||
-        h.version != kCkptVersion || h.header_bytes != sizeof h) {
-        std::fclose(f);
-        return fail(ctx, NS3D_ERR_FILE, std::string("not a version 1 checkpoint: ") + path);
-    }
-    if (h.nx != ctx->p.global_nx || h.ny != ctx->p.global_ny || h.nz != ctx->p.global_nz ||
-        !same_bits(h.dx, ctx->p.dx) || !same_bits(h.dy, ctx->p.dy) || !same_bits(h.dz, ctx->p.dz)) {
-        std::fclose(f);
-        return fail(ctx, NS3D_ERR_INVALID, "the checkpoint's grid differs from the context's");
-    }
+    FILE* f = nullptr;
+    std::string msg;
+    const ns3d_status hs = checkpoint_open(path, &ctx->p, &h, &f, &msg);
+    if (hs != NS3D_OK) return fail(ctx, hs, msg);
     const long long nw = 6 * ctx->n;
     std::vector<double> buf((size_t)nw);
     const size_t got = std::fread(buf.data(), sizeof(double), (size_t)nw, f);
@@ -1149,6 +1274,13 @@ ns3d_status ns3d_checkpoint_read(ns3d_ctx* ctx, const char* path) {
     ctx->rec = ctx->cur;
     ctx->time = h.time;
     ctx->out_next = h.out_next;
+    ctx->steps = h.steps;
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_completed_steps(ns3d_ctx* ctx, long long* steps) {
+    if (!ctx || !steps) return NS3D_ERR_INVALID;
+    *steps = ctx->steps;
     return NS3D_OK;
 }
 
@@ -1172,16 +1304,25 @@ ns3d_status ns3d_energy_spectrum(ns3d_ctx* ctx, double* Ek, int nbins) {
         cufftSetStream(ctx->fft, ctx->stream);
         NS3D_CK(cudaMalloc(&ctx->spec, sizeof(cufftDoubleComplex) * (size_t)(nx / 2 + 1) * ny * nz));
         NS3D_CK(cudaMalloc(&ctx->bins, sizeof(double) * kmax));
+        const int nbu = spectrum_bins_used(nx, ny, nz);
+        NS3D_CK(cudaMalloc(&ctx->spec_part, sizeof(double) * (size_t)SPEC_BLOCKS * nbu));
+        if (sizeof(double) * SPEC_WARPS * nbu > 48 * 1024)
+            NS3D_CK(cudaFuncSetAttribute(k_spectrum_part, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(double) * SPEC_WARPS * nbu)));
         ctx->fft_ready = true;
     }
     NS3D_CK(cudaMemsetAsync(ctx->bins, 0, sizeof(double) * kmax, ctx->stream));
     const double scale = 1.0 / (double)ctx->n;  // EnergySpectrum.cpp:88-96
+    const int nbu = spectrum_bins_used(nx, ny, nz);
     for (int comp = 1; comp <= 3; ++comp) {
         if (cufftExecD2Z(ctx->fft, warr(ctx, ctx->cur, comp), ctx->spec) != CUFFT_SUCCESS)
             return fail(ctx, NS3D_ERR_CUDA, "cufftExecD2Z failed");
-        k_spectrum_bin<<<4 * 148, 256, sizeof(double) * kmax, ctx->stream>>>(ctx->spec, nx, ny, nz,
-                                                                             scale, kmax, ctx->bins);
-        NS3D_CK(cudaGetLastError());
+        NS3D_LAUNCH(NS3D_KERNEL_OTHER, 2,
+                    (k_spectrum_part<<<SPEC_BLOCKS, 32 * SPEC_WARPS,
+                                       sizeof(double) * SPEC_WARPS * nbu, ctx->stream>>>(
+                         ctx->spec, nx, ny, nz, scale, nbu, ctx->spec_part),
+                     k_spectrum_final<<<(nbu + 127) / 128, 128, 0, ctx->stream>>>(
+                         ctx->spec_part, SPEC_BLOCKS, nbu, ctx->bins)));
     }
     NS3D_CK(cudaMemcpyAsync(Ek, ctx->bins, sizeof(double) * nbins, cudaMemcpyDeviceToHost, ctx->stream));
     NS3D_CK(cudaStreamSynchronize(ctx->stream));

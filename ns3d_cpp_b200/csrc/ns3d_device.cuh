@@ -171,10 +171,14 @@ __device__ __forceinline__ double sqrt_nr(double b) {
 }
 
 // raw = (rho, u, v, w, p) of one cell; inv_gm1 = 1/(gamma-1), inv_2g = 1/(2 gamma).
+// The face normal (N1, N2, N3) is a coordinate axis, so the normal velocity is
+// one component and the c-terms enter only the normal momentum; the products
+// with the zero components (which IEEE arithmetic cannot drop by itself) are
+// left out.
 template <int FVS, int N1, int N2, int N3, int STEPS = 1>
 __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, double inv_2g,
                                            const double* raw, double Fp[5], double Fm[5]) {
-    const double n1 = N1, n2 = N2, n3 = N3;
+    static_assert(N1 + N2 + N3 == 1, "axis-aligned face normal");
     double rho = raw[0];
     if (rho <= 0.0) rho = 1e-12;
     const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
@@ -183,7 +187,7 @@ __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, d
     const double kinetic = 0.5 * (u * u + v * v + w * w);
     const double E = rho * (p * ir * inv_gm1 + kinetic);
     const double c = sqrt_nr<STEPS>(gamma * p * ir);
-    const double un = u * n1 + v * n2 + w * n3;
+    const double un = N1 ? u : (N2 ? v : w);
     if constexpr (FVS == FV_SW) {
         const double eps = P.sw_eps;
         const double l1 = un - c, l2 = un, l3 = un + c;
@@ -198,18 +202,36 @@ __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, d
         const double H = (E + p) * ir;
         const double ga1 = rho * inv_2g;
         const double ga2 = 2.0 * (gamma - 1.0);
-        Fp[0] = ga1 * (S1p + ga2 * l2p);
-        Fp[1] = ga1 * (S1p * u + ga2 * l2p * u + S2p * n1 * c);
-        Fp[2] = ga1 * (S1p * v + ga2 * l2p * v + S2p * n2 * c);
-        Fp[3] = ga1 * (S1p * w + ga2 * l2p * w + S2p * n3 * c);
-        Fp[4] = ga1 * (S1p * H + ga2 * l2p * kinetic + S2p * un * c);
-        Fm[0] = ga1 * (S1m + ga2 * l2m);
-        Fm[1] = ga1 * (S1m * u + ga2 * l2m * u + S2m * n1 * c);
-        Fm[2] = ga1 * (S1m * v + ga2 * l2m * v + S2m * n2 * c);
-        Fm[3] = ga1 * (S1m * w + ga2 * l2m * w + S2m * n3 * c);
-        Fm[4] = ga1 * (S1m * H + ga2 * l2m * kinetic + S2m * un * c);
+        const double cp = S2p * c, cm = S2m * c;
+        const double bp = S1p + ga2 * l2p, bm = S1m + ga2 * l2m;  // common factor of u, v, w
+        Fp[0] = ga1 * bp;
+        Fp[1] = ga1 * (N1 ? bp * u + cp : bp * u);
+        Fp[2] = ga1 * (N2 ? bp * v + cp : bp * v);
+        Fp[3] = ga1 * (N3 ? bp * w + cp : bp * w);
+        Fp[4] = ga1 * (S1p * H + ga2 * l2p * kinetic + cp * un);
+        Fm[0] = ga1 * bm;
+        Fm[1] = ga1 * (N1 ? bm * u + cm : bm * u);
+        Fm[2] = ga1 * (N2 ? bm * v + cm : bm * v);
+        Fm[3] = ga1 * (N3 ? bm * w + cm : bm * w);
+        Fm[4] = ga1 * (S1m * H + ga2 * l2m * kinetic + cm * un);
     } else {
-        split_lf<double, N1, N2, N3>(rho, u, v, w, E, p, c, Fp, Fm);
+        // split_lf with the pressure only in the normal momentum
+        const double a_max = fabs(un) + c;
+        const double F1 = rho * un;
+        const double F2 = rho * u * un + (N1 ? p : 0.0);
+        const double F3 = rho * v * un + (N2 ? p : 0.0);
+        const double F4 = rho * w * un + (N3 ? p : 0.0);
+        const double F5 = (E + p) * un;
+        Fp[0] = 0.5 * (F1 + a_max * rho);
+        Fp[1] = 0.5 * (F2 + a_max * rho * u);
+        Fp[2] = 0.5 * (F3 + a_max * rho * v);
+        Fp[3] = 0.5 * (F4 + a_max * rho * w);
+        Fp[4] = 0.5 * (F5 + a_max * E);
+        Fm[0] = 0.5 * (F1 - a_max * rho);
+        Fm[1] = 0.5 * (F2 - a_max * rho * u);
+        Fm[2] = 0.5 * (F3 - a_max * rho * v);
+        Fm[3] = 0.5 * (F4 - a_max * rho * w);
+        Fm[4] = 0.5 * (F5 - a_max * E);
     }
 }
 
@@ -274,6 +296,18 @@ __device__ __forceinline__ void eigen_LR(double gamma, const double* ua, double 
 // reversal that reconstruct_select applies for the minus flux (:24-31).
 // ---------------------------------------------------------------------------
 
+// a / b for a divisor b known in advance, with y = RN(1/b) precomputed (an IEEE
+// division): Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990)
+// -- if y is 1/b correctly rounded and q is within one ulp of a/b, then
+// r = a - b q is a double (one exact FMA) and RN(q + r y) = RN(a/b). Here
+// q = RN(a y) is within one ulp, so the result equals the IEEE quotient a / b
+// bit for bit (finite a/b in the normal range), in three operations.
+__device__ __forceinline__ double div_rcp(double a, double b, double y) {
+    const double q = a * y;
+    const double r = fma(-b, q, a);
+    return fma(r, y, q);
+}
+
 // weno5_reconstruction (reconstruction.cpp:93-124): WENO5-JS, eps 1e-6, p = 2.
 template <class R>
 __device__ __forceinline__ R weno5(R f0, R f1, R f2, R f3, R f4) {
@@ -291,18 +325,26 @@ __device__ __forceinline__ R weno5(R f0, R f1, R f2, R f3, R f4) {
     R w0 = alpha0 / asum;
     R w1 = alpha1 / asum;
     R w2 = alpha2 / asum;
-    R p0 = (R(2) * f0 - R(7) * f1 + R(11) * f2) / R(6.0);
-    R p1 = (-f1 + R(5) * f2 + R(2) * f3) / R(6.0);
-    R p2 = (R(2) * f2 + R(5) * f3 - f4) / R(6.0);
+    // the reference's division by 6, as the IEEE quotient (div_rcp)
+    const double six = 6.0, rcp6 = 1.0 / 6.0;
+    R p0 = div_rcp(R(2) * f0 - R(7) * f1 + R(11) * f2, six, rcp6);
+    R p1 = div_rcp(-f1 + R(5) * f2 + R(2) * f3, six, rcp6);
+    R p2 = div_rcp(R(2) * f2 + R(5) * f3 - f4, six, rcp6);
     return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
 // FP32-stencil form of weno5 (preferred over the template for float): the same
-// indicators, weights and normalised sum, with approximate divisions for the
-// weights, one reciprocal of their sum and the 1/6 as a multiplication. It
-// gives the same FP32-vs-FP64 error as the template at 7% less sweep time;
-// folding the normalisation and the 1/6 into one final division instead was
-// measured 4x further from the FP64 form after 100 steps at 256^3.
+// indicators z_k = eps + beta_k and the same normalised combination of the
+// three candidate stencils, with the nonlinear weights taken over a common
+// denominator. With y_k = z_k^2, alpha_k = d_k / y_k; multiplying every
+// alpha_k by y0 y1 y2 gives e_k = d_k m_k (m0 = y1 y2, m1 = y0 y2, m2 = y0 y1)
+// and w_k = e_k / (e0 + e1 + e2): one reciprocal per reconstruction instead
+// of four divisions. z_k >= eps = 1e-6, so the products stay >= 1e-25, well
+// inside float's normal range for any deviation below ~1e4. The candidate
+// stencils keep their integer coefficients (summing to exactly 6) and the 1/6
+// is applied once to the combination: coefficients pre-divided by 6 do not sum
+// to 1 in float and were measured to bias the faces by the deviation's size.
+__device__ __forceinline__ float rcp_approx(float x);
 __device__ __forceinline__ float weno5(float f0, float f1, float f2, float f3, float f4) {
     const float eps = 1e-6f;
     const float t0 = f0 - 2.f * f1 + f2, s0 = f0 - 4.f * f1 + 3.f * f2;
@@ -311,15 +353,13 @@ __device__ __forceinline__ float weno5(float f0, float f1, float f2, float f3, f
     const float z0 = eps + ((13.f / 12.f) * t0 * t0 + 0.25f * s0 * s0);
     const float z1 = eps + ((13.f / 12.f) * t1 * t1 + 0.25f * s1 * s1);
     const float z2 = eps + ((13.f / 12.f) * t2 * t2 + 0.25f * s2 * s2);
-    const float a0 = __fdividef(0.1f, z0 * z0);
-    const float a1 = __fdividef(0.6f, z1 * z1);
-    const float a2 = __fdividef(0.3f, z2 * z2);
-    const float inv = __fdividef(1.f, a0 + a1 + a2);
-    const float w0 = a0 * inv, w1 = a1 * inv, w2 = a2 * inv;
-    const float p0 = (2.f * f0 - 7.f * f1 + 11.f * f2) * (1.f / 6.f);
-    const float p1 = (-f1 + 5.f * f2 + 2.f * f3) * (1.f / 6.f);
-    const float p2 = (2.f * f2 + 5.f * f3 - f4) * (1.f / 6.f);
-    return w0 * p0 + w1 * p1 + w2 * p2;
+    const float y0 = z0 * z0, y1 = z1 * z1, y2 = z2 * z2;
+    const float e0 = 0.1f * (y1 * y2), e1 = 0.6f * (y0 * y2), e2 = 0.3f * (y0 * y1);
+    const float P0 = 2.f * f0 - 7.f * f1 + 11.f * f2;
+    const float P1 = -f1 + 5.f * f2 + 2.f * f3;
+    const float P2 = 2.f * f2 + 5.f * f3 - f4;
+    const float num = e0 * P0 + e1 * P1 + e2 * P2;
+    return (num * (1.f / 6.f)) * rcp_approx(e0 + e1 + e2);
 }
 
 // Approximate float reciprocal (the hardware estimate, ~1 ulp).
@@ -331,10 +371,10 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 // Two float weno5 reconstructions at once in sm_100's paired FP32 arithmetic
 // (one FFMA2/FADD2/FMUL2 instruction per operation on both lanes of a float2):
-// the same indicators, weights, candidate stencils and normalised sum as
-// weno5(float), operation for operation; only the approximate reciprocals run
-// per lane. The sweeps are instruction-issue bound, so halving the
-// reconstructions' instruction count shortens them.
+// the same indicators, common-denominator weights, candidate stencils and
+// normalised sum as weno5(float), operation for operation; only the one
+// approximate reciprocal runs per lane. The sweeps are instruction-issue
+// bound, so halving the reconstructions' instruction count shortens them.
 __device__ __forceinline__ float2 weno5x2(float2 f0, float2 f1, float2 f2, float2 f3, float2 f4) {
     auto c = [](float v) { return make_float2(v, v); };
     const float2 t0 = __fadd2_rn(__ffma2_rn(c(-2.f), f1, f0), f2);
@@ -351,22 +391,18 @@ __device__ __forceinline__ float2 weno5x2(float2 f0, float2 f1, float2 f2, float
     const float2 z2 = __fadd2_rn(c(1e-6f), __ffma2_rn(__fmul2_rn(c(13.f / 12.f), t2), t2,
                                                       __fmul2_rn(__fmul2_rn(c(0.25f), s2), s2)));
     const float2 y0 = __fmul2_rn(z0, z0), y1 = __fmul2_rn(z1, z1), y2 = __fmul2_rn(z2, z2);
-    const float2 a0 = __fmul2_rn(c(0.1f), make_float2(rcp_approx(y0.x), rcp_approx(y0.y)));
-    const float2 a1 = __fmul2_rn(c(0.6f), make_float2(rcp_approx(y1.x), rcp_approx(y1.y)));
-    const float2 a2 = __fmul2_rn(c(0.3f), make_float2(rcp_approx(y2.x), rcp_approx(y2.y)));
-    const float2 sum = __fadd2_rn(__fadd2_rn(a0, a1), a2);
-    const float2 inv = make_float2(rcp_approx(sum.x), rcp_approx(sum.y));
-    const float2 w0 = __fmul2_rn(a0, inv), w1 = __fmul2_rn(a1, inv), w2 = __fmul2_rn(a2, inv);
-    // integer-coefficient stencils (coefficients summing to exactly 6), then 1/6:
-    // pre-divided coefficients do not sum to 1 in float and were measured to
-    // bias the faces by the deviation's size (4x the error against FP64)
-    const float2 p0 = __fmul2_rn(__ffma2_rn(c(11.f), f2, __ffma2_rn(c(-7.f), f1, __fmul2_rn(c(2.f), f0))),
-                                 c(1.f / 6.f));
-    const float2 p1 = __fmul2_rn(__ffma2_rn(c(2.f), f3, __ffma2_rn(c(5.f), f2, __fmul2_rn(c(-1.f), f1))),
-                                 c(1.f / 6.f));
-    const float2 p2 = __fmul2_rn(__ffma2_rn(c(-1.f), f4, __ffma2_rn(c(5.f), f3, __fmul2_rn(c(2.f), f2))),
-                                 c(1.f / 6.f));
-    return __ffma2_rn(w2, p2, __ffma2_rn(w1, p1, __fmul2_rn(w0, p0)));
+    // e_k = d_k m_k over the common denominator y0 y1 y2 (see weno5(float))
+    const float2 e0 = __fmul2_rn(c(0.1f), __fmul2_rn(y1, y2));
+    const float2 e1 = __fmul2_rn(c(0.6f), __fmul2_rn(y0, y2));
+    const float2 e2 = __fmul2_rn(c(0.3f), __fmul2_rn(y0, y1));
+    const float2 den = __fadd2_rn(__fadd2_rn(e0, e1), e2);
+    // integer-coefficient stencils (coefficients summing to exactly 6), 1/6 once
+    const float2 P0 = __ffma2_rn(c(11.f), f2, __ffma2_rn(c(-7.f), f1, __fmul2_rn(c(2.f), f0)));
+    const float2 P1 = __ffma2_rn(c(2.f), f3, __ffma2_rn(c(5.f), f2, __fmul2_rn(c(-1.f), f1)));
+    const float2 P2 = __ffma2_rn(c(-1.f), f4, __ffma2_rn(c(5.f), f3, __fmul2_rn(c(2.f), f2)));
+    const float2 num = __ffma2_rn(e2, P2, __ffma2_rn(e1, P1, __fmul2_rn(e0, P0)));
+    const float2 inv = make_float2(rcp_approx(den.x), rcp_approx(den.y));
+    return __fmul2_rn(__fmul2_rn(num, c(1.f / 6.f)), inv);
 }
 
 // The 10 WENO5 reconstructions of one face in the FP32 form, paired as

@@ -104,6 +104,83 @@ __device__ __forceinline__ void char_face(double gamma, const double* wl, const 
 }
 
 // ---------------------------------------------------------------------------
+// Split-flux storage of the sweeps in shared memory. A slot holds one cell's
+// split fluxes, FP32: (F+0..3) float4, (F-0..3) float4, (F+4, F-4) float2 --
+// exactly the operand pairs of the paired WENO5; FP64: five double2. The
+// arrays are [slot][t]: threads with consecutive t read consecutive 8- or
+// 16-byte words (no bank conflicts).
+// ---------------------------------------------------------------------------
+template <class R> struct RingCfg;
+template <> struct RingCfg<float> { static constexpr int T = 128, MINB = 4; };
+template <> struct RingCfg<double> { static constexpr int T = 64, MINB = 6; };
+
+template <class R, int S, int T> struct SplitRing;
+template <int S, int T> struct SplitRing<float, S, T> {
+    float4 p[S][T];   // F+0..3
+    float4 m[S][T];   // F-0..3
+    float2 e[S][T];   // F+4, F-4
+    __device__ __forceinline__ void put(int slot, int t, const float* Fp, const float* Fm) {
+        p[slot][t] = make_float4(Fp[0], Fp[1], Fp[2], Fp[3]);
+        m[slot][t] = make_float4(Fm[0], Fm[1], Fm[2], Fm[3]);
+        e[slot][t] = make_float2(Fp[4], Fm[4]);
+    }
+    __device__ __forceinline__ void get(int slot, int t, float* Fp, float* Fm) const {
+        const float4 a = p[slot][t], b = m[slot][t];
+        const float2 c = e[slot][t];
+        Fp[0] = a.x; Fp[1] = a.y; Fp[2] = a.z; Fp[3] = a.w; Fp[4] = c.x;
+        Fm[0] = b.x; Fm[1] = b.y; Fm[2] = b.z; Fm[3] = b.w; Fm[4] = c.y;
+    }
+    // component q of F+ (minus = false) or F- of one slot (one scalar load)
+    __device__ __forceinline__ float comp(int slot, int t, int q, bool minus) const {
+        if (q == 4) return reinterpret_cast<const float*>(&e[slot][t])[minus ? 1 : 0];
+        return reinterpret_cast<const float*>(minus ? &m[slot][t] : &p[slot][t])[q];
+    }
+};
+template <int S, int T> struct SplitRing<double, S, T> {
+    double2 a[S][5][T];   // (F+0,F+1) (F+2,F+3) (F-0,F-1) (F-2,F-3) (F+4,F-4)
+    __device__ __forceinline__ void put(int slot, int t, const double* Fp, const double* Fm) {
+        a[slot][0][t] = make_double2(Fp[0], Fp[1]);
+        a[slot][1][t] = make_double2(Fp[2], Fp[3]);
+        a[slot][2][t] = make_double2(Fm[0], Fm[1]);
+        a[slot][3][t] = make_double2(Fm[2], Fm[3]);
+        a[slot][4][t] = make_double2(Fp[4], Fm[4]);
+    }
+    __device__ __forceinline__ void get(int slot, int t, double* Fp, double* Fm) const {
+        const double2 x0 = a[slot][0][t], x1 = a[slot][1][t], x2 = a[slot][2][t];
+        const double2 x3 = a[slot][3][t], x4 = a[slot][4][t];
+        Fp[0] = x0.x; Fp[1] = x0.y; Fp[2] = x1.x; Fp[3] = x1.y; Fp[4] = x4.x;
+        Fm[0] = x2.x; Fm[1] = x2.y; Fm[2] = x3.x; Fm[3] = x3.y; Fm[4] = x4.y;
+    }
+    __device__ __forceinline__ double comp(int slot, int t, int q, bool minus) const {
+        if (q == 4) return reinterpret_cast<const double*>(&a[slot][4][t])[minus ? 1 : 0];
+        return reinterpret_cast<const double*>(&a[slot][(minus ? 2 : 0) + (q >> 1)][t])[q & 1];
+    }
+};
+
+// The window of phase PH (window position m in slot (PH + m) mod S) into
+// registers; the slots are compile-time, so every load has an immediate offset.
+template <int PH, class R, int S, int T>
+__device__ __forceinline__ void ring_window(const SplitRing<R, S, T>& rg, int t, R fp[][5],
+                                            R fm[][5]) {
+#pragma unroll
+    for (int m = 0; m < S; ++m) rg.get((PH + m) % S, t, fp[m], fm[m]);
+}
+template <class R, int S, int T>
+__device__ __forceinline__ void ring_window_at(int ph, const SplitRing<R, S, T>& rg, int t,
+                                               R fp[][5], R fm[][5]) {
+    switch (ph) {
+    case 0: ring_window<0>(rg, t, fp, fm); break;
+    case 1: ring_window<1 % S>(rg, t, fp, fm); break;
+    case 2: ring_window<2 % S>(rg, t, fp, fm); break;
+    case 3: ring_window<3 % S>(rg, t, fp, fm); break;
+    case 4: ring_window<4 % S>(rg, t, fp, fm); break;
+    case 5: ring_window<5 % S>(rg, t, fp, fm); break;
+    case 6: ring_window<6 % S>(rg, t, fp, fm); break;
+    default: ring_window<7 % S>(rg, t, fp, fm); break;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Inviscid sweep along DIR (du_inviscous, InviscousFlux_new.cpp:4-163, and the
 // divergence of range_kutta.cpp:51-98).
 //
@@ -305,7 +382,7 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     constexpr int S = Stencil<RC>::S;
     constexpr int MID = (S - 1) / 2;
     constexpr bool kDeviation = sizeof(R) < sizeof(double);
-    __shared__ R ring[XW_WARPS][2][5][96];  // [warp][+/-][component][3 chunks x 32]
+    __shared__ SplitRing<R, XW_WARPS, 96> ring;  // [warp][3 chunks x 32 cells]
     const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
     const int nx = P.nx;
     const long long n = P.n;
@@ -364,62 +441,50 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
             refm[q] = __shfl_sync(0xffffffffu, Fmd[q], 0);
         }
     }
-    R (*rp)[96] = ring[wq][0];
-    R (*rm)[96] = ring[wq][1];
-    auto put = [&](int slot, const R* Fp, const R* Fm) {
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            rp[q][slot * 32 + lane] = Fp[q];
-            rm[q][slot * 32 + lane] = Fm[q];
-        }
-    };
+    auto put = [&](int slot, const R* Fp, const R* Fm) { ring.put(wq, slot * 32 + lane, Fp, Fm); };
     // face at chunk-relative position `pos` (face pos sits between cells pos and
     // pos+1 of chunk `chunk`, held in slot `cs`); window cells pos-MID .. pos-MID+S-1
     auto face_at = [&](int cs, int pos, int chunk, R* face) {
-        if constexpr (CHR) {
-            // the face's two cells, loaded coalesced over the warp (rho as stored)
-            auto at = [&](int m) {
-                int k = cs * 32 + pos - MID + m;
-                return k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
-            };
-            int gl = chunk * 32 + pos;
-            gl = gl < 0 ? gl + nx : gl;
-            const int gr = gl + 1 == nx ? 0 : gl + 1;
-            const double wl[5] = {W.rho[base + gl], W.u[base + gl], W.v[base + gl],
-                                  W.w[base + gl], W.p[base + gl]};
-            const double wr[5] = {W.rho[base + gr], W.u[base + gr], W.v[base + gr],
-                                  W.w[base + gr], W.p[base + gr]};
-            char_face<0, R, RC>(P.gamma, wl, wr, [&](int m, int r) { return rp[r][at(m)]; },
-                                [&](int m, int r) { return rm[r][at(m)]; }, lin, disp, diss, face);
-            return;
+        int cell[S];
+#pragma unroll
+        for (int m = 0; m < S; ++m) {
+            const int k = cs * 32 + pos - MID + m;
+            cell[m] = k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
         }
-        if constexpr (kDeviation && RC == RC_WENO5) {
-            auto at = [&](int m) {
-                int k = cs * 32 + pos - MID + m;
-                return k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
-            };
-            weno5_face_x2([&](int m, int q) { return rp[q][at(m)]; },
-                          [&](int m, int q) { return rm[q][at(S - 1 - m)]; }, face);
-            return;
-        }
+        if constexpr (CHR || (kDeviation && RC == RC_WENO5)) {
+            R fp[S][5], fm[S][5];
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            R a[S], b[S];
-#pragma unroll
-            for (int m = 0; m < S; ++m) {
-                int k = cs * 32 + pos - MID + m;
-                k = k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
-                a[m] = rp[q][k];
+            for (int m = 0; m < S; ++m) ring.get(wq, cell[m], fp[m], fm[m]);
+            if constexpr (CHR) {
+                // the face's two cells, loaded coalesced over the warp (rho as stored)
+                int gl = chunk * 32 + pos;
+                gl = gl < 0 ? gl + nx : gl;
+                const int gr = gl + 1 == nx ? 0 : gl + 1;
+                const double wl[5] = {W.rho[base + gl], W.u[base + gl], W.v[base + gl],
+                                      W.w[base + gl], W.p[base + gl]};
+                const double wr[5] = {W.rho[base + gr], W.u[base + gr], W.v[base + gr],
+                                      W.w[base + gr], W.p[base + gr]};
+                char_face<0, R, RC>(P.gamma, wl, wr, [&](int m, int r) { return fp[m][r]; },
+                                    [&](int m, int r) { return fm[m][r]; }, lin, disp, diss,
+                                    face);
+            } else {
+                weno5_face_x2([&](int m, int q) { return fp[m][q]; },
+                              [&](int m, int q) { return fm[S - 1 - m][q]; }, face);
             }
+        } else {
+            // scalar reconstructions: one component of the window at a time
 #pragma unroll
-            for (int m = 0; m < S; ++m) {
-                int k = cs * 32 + pos - MID + (S - 1 - m);
-                k = k < 0 ? k + 96 : (k >= 96 ? k - 96 : k);
-                b[m] = rm[q][k];
+            for (int q = 0; q < 5; ++q) {
+                R a[S], b[S];
+#pragma unroll
+                for (int m = 0; m < S; ++m) {
+                    a[m] = ring.comp(wq, cell[m], q, false);
+                    b[m] = ring.comp(wq, cell[S - 1 - m], q, true);
+                }
+                const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+                const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+                face[q] = plus_face + minus_face;
             }
-            const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
-            const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
-            face[q] = plus_face + minus_face;
         }
     };
 
@@ -679,12 +744,11 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
     }
 }
 
-// rhs at one cell: compute_vis_flux (ViscousFlux.cpp:370-384, x then y then z
-// added to 0) followed by the inviscid divergence (range_kutta.cpp:61-97).
+// Viscous part of the rhs at one cell: compute_vis_flux (ViscousFlux.cpp:370-384,
+// x then y then z added to 0); r[0] = 0.
 template <class R, int ORD>
-__device__ __forceinline__ void cell_rhs(const DevParams& P, const R* __restrict__ tacc,
-                                         const R* __restrict__ fv, int i, int j, int k,
-                                         long long id, R r[5]) {
+__device__ __forceinline__ void cell_visc(const DevParams& P, const R* __restrict__ fv, int i,
+                                          int j, int k, long long id, R r[5]) {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const long long n = P.n, sxy = (long long)nx * ny;
     const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
@@ -735,6 +799,16 @@ __device__ __forceinline__ void cell_rhs(const DevParams& P, const R* __restrict
             r[m + 1] = acc;
         }
     }
+}
+
+// rhs at one cell: the viscous part followed by the inviscid divergence
+// (range_kutta.cpp:61-97) accumulated in tacc.
+template <class R, int ORD>
+__device__ __forceinline__ void cell_rhs(const DevParams& P, const R* __restrict__ tacc,
+                                         const R* __restrict__ fv, int i, int j, int k,
+                                         long long id, R r[5]) {
+    cell_visc<R, ORD>(P, fv, i, j, k, id, r);
+    const long long n = P.n;
 #pragma unroll
     for (int q = 0; q < 5; ++q) r[q] += -tacc[q * n + id];
 }
@@ -926,6 +1000,208 @@ k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
     if (STAGE == 3) block_min_to(cand, &ctrl->dtmin_bits);
 }
 
+// ---------------------------------------------------------------------------
+// y and z sweeps with the face window in shared memory (component-wise
+// reconstruction; du_inviscous, InviscousFlux_new.cpp:4-163, and the
+// divergence of range_kutta.cpp:51-98).
+//
+// Same march as k_sweep (one thread per line segment, threads over x, every
+// cell split once, one reconstruction per face), but the split fluxes of the
+// S window cells sit in a per-thread ring of S shared-memory slots instead of
+// registers: the new cell's split overwrites the slot of the cell that left
+// the window, so nothing is shifted per step (the register window cost 10(S-1)
+// moves per cell) and the ~10 S registers of the window are freed for more
+// resident warps. Each thread touches only its own column of the ring, so no
+// barrier is needed.
+//
+// FUSE (z sweep only): after the z difference of a cell, the rest of the
+// stage runs on it in the same thread -- the viscous divergence of the fluxes
+// fv, rhs = visc + (-(T_acc + az idz)) in the reference's order, the
+// Shu-Osher stage, conservedToPrimitive and (stage 3) positivity and the next
+// step's CFL candidates -- so T_acc's z term is never stored and the
+// memory-bound update runs under the compute-bound sweep. Results equal
+// k_sweep<2> followed by k_update bit for bit.
+// ---------------------------------------------------------------------------
+
+// Stage-update operands of the fused z sweep.
+template <class R>
+struct FuseArgs {
+    int stage;            // 1, 2, 3
+    StateView W0;         // recorded state (U0 = prim2cons(W0))
+    const R* fv;          // viscous fluxes (store_fv layout)
+    StateOut Wn;          // output state
+    Ctrl* ctrl;           // dt, bad_cell, dtmin_bits
+};
+
+template <class R, int STAGE>
+__device__ __forceinline__ void fused_cell(const DevParams& P, const StateView& Wc,
+                                           const FuseArgs<R>& F, int i, int j, int k,
+                                           long long id, const R tz[5], double dt, double& cand) {
+    R r[5];
+    if (P.vis_order == 4) cell_visc<R, 4>(P, F.fv, i, j, k, id, r);
+    else if (P.vis_order == 6) cell_visc<R, 6>(P, F.fv, i, j, k, id, r);
+    else cell_visc<R, 8>(P, F.fv, i, j, k, id, r);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) r[q] += -tz[q];
+    stage_cell<R, STAGE>(P, Wc, F.W0, id, r, dt, F.Wn, F.ctrl, cand);
+}
+
+template <int DIR, class R, int FVS, int RC, bool FUSE>
+__global__ void __launch_bounds__(RingCfg<R>::T, RingCfg<R>::MINB)
+k_sweep_ring(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __restrict__ ctrl,
+             FuseArgs<R> F) {
+    static_assert(DIR == 1 || DIR == 2, "y and z sweeps");
+    static_assert(!FUSE || DIR == 2, "the stage update follows the last (z) sweep");
+    constexpr int S = Stencil<RC>::S;
+    constexpr int MID = (S - 1) / 2;
+    constexpr int T = RingCfg<R>::T;
+    constexpr bool kDeviation = sizeof(R) < sizeof(double);
+    __shared__ SplitRing<R, S, T> ring;
+    if (ctrl && ctrl->stop) return;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = P.n;
+    const int tid = threadIdx.x;
+    const int t0 = blockIdx.x * blockDim.x + tid;
+    const bool live = t0 < nx;
+    const int len = DIR == 1 ? ny : nz;
+    const long long stride = DIR == 1 ? (long long)nx : (long long)nx * ny;
+    const long long base = DIR == 1 ? (long long)blockIdx.y * ny * nx + (live ? t0 : 0)
+                                    : (long long)blockIdx.y * nx + (live ? t0 : 0);
+    const int c0 = blockIdx.z * seg;
+    if (c0 >= len) return;  // block-uniform
+    const int c1 = min(c0 + seg, len);
+
+    R lin[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) lin[m] = R(P.lin[m]);
+    const R disp = R(P.mdcd_disp), diss = R(P.mdcd_diss);
+    const R inv_h = R(DIR == 1 ? P.inv_dy : P.inv_dz);
+    const R gamma = R(P.gamma), eps = R(P.sw_eps);
+    (void)gamma;
+    (void)eps;
+    double refp[5], refm[5];
+    const double inv_gm1 = kDeviation ? 1.0 / (P.gamma - 1.0) : 0.0;
+    const double inv_2g = kDeviation ? 1.0 / (2.0 * P.gamma) : 0.0;
+    auto load_raw = [&](int s, double* raw) {
+        const long long id = base + (long long)wrap1(s, len) * stride;
+        raw[0] = W.rho[id];
+        raw[1] = W.u[id];
+        raw[2] = W.v[id];
+        raw[3] = W.w[id];
+        raw[4] = W.p[id];
+    };
+    // the split of k_sweep (FP32 form: double split, minus the segment's first
+    // cell's split flux, rounded to float)
+    auto split_raw = [&](const double* raw, R* Fp, R* Fm, bool set_ref) {
+        if constexpr (!kDeviation) {
+            R rr = R(raw[0]);
+            const R u = R(raw[1]), v = R(raw[2]), w = R(raw[3]), p = R(raw[4]);
+            if (rr <= R(0)) rr = R(1e-12);
+            R E, c;
+            p2c_Ec(rr, u, v, w, p, gamma, E, c);
+            if constexpr (FVS == FV_SW)
+                split_sw<R, 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, gamma, eps, Fp, Fm);
+            else
+                split_lf<R, 0, DIR == 1, DIR == 2>(rr, u, v, w, E, p, c, Fp, Fm);
+        } else {
+            double Fpd[5], Fmd[5];
+            split_fast<FVS, 0, DIR == 1, DIR == 2>(P, inv_gm1, inv_2g, raw, Fpd, Fmd);
+            if (set_ref) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    refp[q] = Fpd[q];
+                    refm[q] = Fmd[q];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                Fp[q] = R(Fpd[q] - refp[q]);
+                Fm[q] = R(Fmd[q] - refm[q]);
+            }
+        }
+    };
+
+    double cand = CFL_INIT;
+    double dt = 0.0;
+    if constexpr (FUSE) dt = F.ctrl->dt;
+    if (live) {
+        int f = c0 - 1;  // face f sits between cells f and f+1
+        double nxt[5];
+#pragma unroll
+        for (int m = 0; m < S - 1; ++m) {
+            load_raw(f - MID + m, nxt);
+            R Fp[5], Fm[5];
+            split_raw(nxt, Fp, Fm, m == 0);
+            ring.put(m, tid, Fp, Fm);
+        }
+        load_raw(f - MID + S - 1, nxt);
+        R prev[5];
+        int ph = 0;  // window position m of this face sits in slot (ph + m) mod S
+        for (int t = 0; f < c1; ++t, ++f) {
+            double cur[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) cur[q] = nxt[q];
+            load_raw(f - MID + S, nxt);  // the following cell, one step ahead
+            const long long oid = base + (long long)f * stride;
+            R old[5];
+            if (t > 0) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) old[q] = tacc[q * n + oid];
+            }
+            {
+                R Fp[5], Fm[5];
+                split_raw(cur, Fp, Fm, false);
+                ring.put(ph == 0 ? S - 1 : ph - 1, tid, Fp, Fm);
+            }
+            R face[5];
+            if constexpr (kDeviation && RC == RC_WENO5) {
+                R fp[S][5], fm[S][5];
+                ring_window_at(ph, ring, tid, fp, fm);
+                // reconstruct_select reverses the minus window (flag < 0)
+                weno5_face_x2([&](int m, int q) { return fp[m][q]; },
+                              [&](int m, int q) { return fm[S - 1 - m][q]; }, face);
+            } else {
+                // scalar reconstructions: one component of the window at a time
+                int sl[S];
+#pragma unroll
+                for (int m = 0; m < S; ++m) sl[m] = ph + m < S ? ph + m : ph + m - S;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    R a[S], b[S];
+#pragma unroll
+                    for (int m = 0; m < S; ++m) {
+                        a[m] = ring.comp(sl[m], tid, q, false);
+                        b[m] = ring.comp(sl[S - 1 - m], tid, q, true);
+                    }
+                    const R plus_face = reconstruct<R, RC>(a, lin, disp, diss);
+                    const R minus_face = reconstruct<R, RC>(b, lin, disp, diss);
+                    face[q] = plus_face + minus_face;
+                }
+            }
+            if (t > 0) {
+                R tz[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) tz[q] = old[q] + (face[q] - prev[q]) * inv_h;
+                if constexpr (FUSE) {
+                    const int i = t0, j = blockIdx.y;
+                    if (F.stage == 1) fused_cell<R, 1>(P, W, F, i, j, f, oid, tz, dt, cand);
+                    else if (F.stage == 2) fused_cell<R, 2>(P, W, F, i, j, f, oid, tz, dt, cand);
+                    else fused_cell<R, 3>(P, W, F, i, j, f, oid, tz, dt, cand);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) tacc[q * n + oid] = tz[q];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 5; ++q) prev[q] = face[q];
+            ph = ph + 1 == S ? 0 : ph + 1;
+        }
+    }
+    if constexpr (FUSE) {
+        if (F.stage == 3) block_min_to(cand, &F.ctrl->dtmin_bits);
+    }
+}
+
 // Sums of the reductions below (see k_sums_partial).
 constexpr int NSUMS = 13;
 
@@ -961,7 +1237,6 @@ __global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, do
     }
     double dt = dt_fixed;
     if (dt_fixed < 0.0) dt = cfl * __longlong_as_double((long long)c->dtmin_bits);
-    c->dtmin_bits = pos_double_bits(CFL_INIT);
     if (mode >= 1) {
         double t = c->time;
         if (t >= c->out_next - eps) {
@@ -975,6 +1250,7 @@ __global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, do
             c->output = 1;
         }
         if (dt <= eps) {
+            // the state is unchanged: its CFL minimum stays valid
             c->stop = 1;
             c->stop_reason = STOP_DT_SMALL;
             c->stop_in_pre = 1;
@@ -982,6 +1258,8 @@ __global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, do
             return;
         }
     }
+    // the step runs: its stage 3 collects the next state's CFL minimum
+    c->dtmin_bits = pos_double_bits(CFL_INIT);
     c->time += dt;
     c->dt = dt;
     c->active = 1;

@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "ns3d_kernels.cuh"
 
 namespace ns3d {
@@ -33,6 +35,12 @@ cudaError_t launch_update(const LaunchCfg& L, int stage, StateView Wc, StateView
                           const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl);
 template <class R>
 cudaError_t launch_rhs_out(const LaunchCfg& L, const R* tacc, const R* fv, double* rhs);
+// The z sweep fused with the stage update (k_sweep_ring<2, ..., FUSE>): T_acc
+// holds the x + y terms, fv the viscous fluxes of Wc; writes Wn. Component-wise
+// reconstruction only (L.chr == 0; cudaErrorNotSupported otherwise).
+template <class R>
+cudaError_t launch_sweep_z_update(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
+                                  const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl);
 
 namespace detail {
 
@@ -56,6 +64,26 @@ inline int segment_for(int len, long long lines) {
 
 namespace detail {
 
+// Launch shape of a marching sweep along DIR (threads over the line index of
+// `ext`, blockIdx.y over `other`, blockIdx.z over segments of `seg` cells).
+struct MarchShape {
+    dim3 grid;
+    int th, seg;
+};
+template <int DIR>
+inline MarchShape march_shape(const LaunchCfg& L, int max_threads) {
+    const DevParams& P = L.P;
+    const int ext = DIR == 0 ? P.ny : P.nx;        // thread dimension
+    const int other = DIR == 2 ? P.ny : P.nz;     // blockIdx.y dimension
+    const int len = DIR == 0 ? P.nx : (DIR == 1 ? P.ny : P.nz);
+    MarchShape m;
+    m.seg = L.seg[DIR] > 0 ? L.seg[DIR] : segment_for(len, (long long)ext * other);
+    m.th = threads_for(ext);
+    if (m.th > max_threads) m.th = max_threads;
+    m.grid = dim3((ext + m.th - 1) / m.th, other, (len + m.seg - 1) / m.seg);
+    return m;
+}
+
 template <int DIR, class R, int FVS, int RC, bool CHR>
 cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl) {
     const DevParams& P = L.P;
@@ -65,13 +93,24 @@ cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl
         k_sweep_x_warp<R, FVS, RC, CHR><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
         return cudaGetLastError();
     }
-    const int ext = DIR == 0 ? P.ny : P.nx;        // thread dimension
-    const int other = DIR == 2 ? P.ny : P.nz;     // blockIdx.y dimension
-    const int len = DIR == 0 ? P.nx : (DIR == 1 ? P.ny : P.nz);
-    const int seg = L.seg[DIR] > 0 ? L.seg[DIR] : segment_for(len, (long long)ext * other);
-    const int th = threads_for(ext);
-    dim3 grid((ext + th - 1) / th, other, (len + seg - 1) / seg);
-    k_sweep<DIR, R, FVS, RC, CHR><<<grid, th, 0, L.stream>>>(P, W, tacc, seg, ctrl);
+    if constexpr (DIR != 0 && !CHR) {
+        const MarchShape m = march_shape<DIR>(L, RingCfg<R>::T);
+        k_sweep_ring<DIR, R, FVS, RC, false><<<m.grid, m.th, 0, L.stream>>>(
+            P, W, tacc, m.seg, ctrl, FuseArgs<R>{});
+        return cudaGetLastError();
+    } else {
+        const MarchShape m = march_shape<DIR>(L, 128);
+        k_sweep<DIR, R, FVS, RC, CHR><<<m.grid, m.th, 0, L.stream>>>(P, W, tacc, m.seg, ctrl);
+        return cudaGetLastError();
+    }
+}
+
+template <class R, int FVS, int RC>
+cudaError_t sweep_z_update(const LaunchCfg& L, const FuseArgs<R>& F, StateView Wc,
+                           const R* tacc) {
+    const MarchShape m = march_shape<2>(L, RingCfg<R>::T);
+    k_sweep_ring<2, R, FVS, RC, true><<<m.grid, m.th, 0, L.stream>>>(
+        L.P, Wc, const_cast<R*>(tacc), m.seg, F.ctrl, F);
     return cudaGetLastError();
 }
 
@@ -106,6 +145,26 @@ template <class R>
 cudaError_t launch_sweep(const LaunchCfg& L, int dir, StateView W, R* tacc, const Ctrl* ctrl) {
     return L.fvs == FV_SW ? detail::sweeps_rc<R, FV_SW>(L, dir, W, tacc, ctrl)
                           : detail::sweeps_rc<R, FV_LF>(L, dir, W, tacc, ctrl);
+}
+
+template <class R>
+cudaError_t launch_sweep_z_update(const LaunchCfg& L, int stage, StateView Wc, StateView W0,
+                                  const R* tacc, const R* fv, StateOut Wn, Ctrl* ctrl) {
+    if (L.chr) return cudaErrorNotSupported;
+    const FuseArgs<R> F{stage, W0, fv, Wn, ctrl};
+    auto by_rc = [&](auto fvs) -> cudaError_t {
+        constexpr int FVS = decltype(fvs)::value;
+        switch (L.rc) {
+        case RC_WENO5: return detail::sweep_z_update<R, FVS, RC_WENO5>(L, F, Wc, tacc);
+        case RC_LINEAR: return detail::sweep_z_update<R, FVS, RC_LINEAR>(L, F, Wc, tacc);
+        case RC_LIN6: return detail::sweep_z_update<R, FVS, RC_LIN6>(L, F, Wc, tacc);
+        case RC_MDCD_HYBRID: return detail::sweep_z_update<R, FVS, RC_MDCD_HYBRID>(L, F, Wc, tacc);
+        case RC_LIN8: return detail::sweep_z_update<R, FVS, RC_LIN8>(L, F, Wc, tacc);
+        default: return cudaErrorInvalidValue;
+        }
+    };
+    return L.fvs == FV_SW ? by_rc(std::integral_constant<int, FV_SW>{})
+                          : by_rc(std::integral_constant<int, FV_LF>{});
 }
 
 namespace detail {
@@ -189,7 +248,9 @@ cudaError_t launch_rhs_out(const LaunchCfg& L, const R* tacc, const R* fv, doubl
     template cudaError_t launch_visc_flux<R>(const LaunchCfg&, StateView, R*, const Ctrl*);    \
     template cudaError_t launch_update<R>(const LaunchCfg&, int, StateView, StateView,         \
                                           const R*, const R*, StateOut, Ctrl*);                \
-    template cudaError_t launch_rhs_out<R>(const LaunchCfg&, const R*, const R*, double*);
+    template cudaError_t launch_rhs_out<R>(const LaunchCfg&, const R*, const R*, double*);   \
+    template cudaError_t launch_sweep_z_update<R>(const LaunchCfg&, int, StateView, StateView, \
+                                                  const R*, const R*, StateOut, Ctrl*);
 
 #endif  // NS3D_LAUNCH_IMPL
 

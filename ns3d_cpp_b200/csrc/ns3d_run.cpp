@@ -116,7 +116,9 @@ extern "C" ns3d_status ns3d_run(ns3d_ctx* ctx, const char* workdir, int max_step
     }
     const Clock::time_point t_start = Clock::now();
     Clock::time_point t_last = t_start;
-    int step = 0;
+    long long done0 = 0;
+    if ((s = ns3d_completed_steps(ctx, &done0)) != NS3D_OK) return s;
+    int step = (int)done0;  // a continued run numbers on (max_steps is the last step number)
     double t = 0.0;
     while (step < max_steps) {
         const int n = std::min(next_monitor(step, m.p.monitor_Stepfreq), max_steps) - step;
@@ -138,6 +140,6 @@ extern "C" ns3d_status ns3d_run(ns3d_ctx* ctx, const char* workdir, int max_step
         std::printf("Simulation complete. Total time: %g s\n",
                     std::chrono::duration<double>(Clock::now() - t_start).count());
     if (time) *time = t;
-    if (steps_done) *steps_done = step;
+    if (steps_done) *steps_done = step - (int)done0;
     return s;
 }

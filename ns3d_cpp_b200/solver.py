@@ -299,7 +299,8 @@ class Solver:
         return grad, J.value, (dts_out if din is None else din)
 
     # -- instrumentation ----------------------------------------------------
-    KERNEL_CLASSES = ("sweep_x", "sweep_y", "sweep_z", "visc_flux", "update", "other")
+    KERNEL_CLASSES = ("sweep_x", "sweep_y", "sweep_z", "visc_flux", "update", "other",
+                      "sweep_z_update")
 
     def stream_handle(self) -> int:
         """The cudaStream_t (as an int) all kernels of this context run on."""
@@ -311,8 +312,8 @@ class Solver:
         self._ck(self.lib.ns3d_profile(self.ctx, int(bool(enable))))
 
     def profile_read(self) -> dict:
-        ms = (ctypes.c_double * 6)()
-        n = (ctypes.c_longlong * 6)()
+        ms = (ctypes.c_double * len(self.KERNEL_CLASSES))()
+        n = (ctypes.c_longlong * len(self.KERNEL_CLASSES))()
         self._ck(self.lib.ns3d_profile_read(self.ctx, ms, n))
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
 

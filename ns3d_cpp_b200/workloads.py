@@ -60,7 +60,8 @@ def _kernel_bytes(cls: str, rsize: int) -> float:
     fv = 12 if rsize == 4 else 9   # viscous flux values per cell (FP32: three float4 blocks)
     return {"sweep_x": w + 5 * rsize, "sweep_y": w + 10 * rsize, "sweep_z": w + 10 * rsize,
             "visc_flux": 32 + fv * rsize,
-            "update": (5.0 / 3.0) * w + (5 + fv) * rsize + 48}.get(cls, 0.0)  # stage 1 reads one state
+            "update": (5.0 / 3.0) * w + (5 + fv) * rsize + 48,  # stage 1 reads one state
+            "sweep_z_update": (5.0 / 3.0) * w + (5 + fv) * rsize + 48}.get(cls, 0.0)
 
 
 def params_for(w: dict, recon: str, precision: str, dt_fixed: float = -1.0) -> SolverParams:

@@ -27,7 +27,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libns3d_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libns3d_ref.so")
-REF_DIR = "/root/reference"
+# the reference's source tree, for building oracle/_ref: the build() argument,
+# else $NS3D_REF_DIR; without either only the C restatement is built
+REF_DIR = os.environ.get("NS3D_REF_DIR", "")
 
 # reference enum orders, field_structures.h:112-131
 FVS = {"stagerwarming": 0, "laxfriedrichs": 1}
@@ -37,17 +39,21 @@ VIS = {"c8th": 0, "c6th": 1, "c4th": 2}
 SUTHERLAND_REF = 110.4 / 288.15          # field_structures.h:100
 
 
-def build(ref: bool | None = None) -> None:
-    """Compile the restatement (always) and the reference build (when its tree exists)."""
+def build(ref: bool | None = None, ref_dir: str | None = None) -> None:
+    """Compile the restatement (always) and the reference build (when the
+    reference tree `ref_dir`, or $NS3D_REF_DIR, exists)."""
+    ref_dir = ref_dir or REF_DIR
     targets = ["oracle"]
     if ref is None:
-        ref = os.path.isdir(REF_DIR)
+        ref = bool(ref_dir) and os.path.isdir(ref_dir)
+    args = ["make", "-s", "-C", HERE, "-j8"]
     if ref:
         targets.append("ref")
         gpu_lib = os.path.join(os.path.dirname(HERE), "ns3d_cpp_b200", "libns3d_b200.so")
         if os.path.exists(gpu_lib):
             targets.append("refgpu")
-    subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={REF_DIR}", "-j8", *targets], check=True)
+        args.append(f"REF_DIR={ref_dir}")
+    subprocess.run(args + targets, check=True)
 
 
 def have_ref() -> bool:

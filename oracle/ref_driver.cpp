@@ -75,6 +75,20 @@ int guarded(RefCtx *c, Fn fn) {
 
 }  // namespace
 
+// The Field3D shim (ns3d_cpp_b200/shim), when this driver is linked into the
+// reference build that uses it, keeps the state on the GPU: host reads of
+// Field3D sync it first, host writes invalidate the device copy. Weak, so the
+// plain reference build (no shim) links without them.
+void ns3d_shim_sync(Field3D &F) __attribute__((weak));
+void ns3d_shim_invalidate(const Field3D &F) __attribute__((weak));
+
+static void host_reads(Field3D &F) {
+    if (ns3d_shim_sync) ns3d_shim_sync(F);
+}
+static void host_wrote(const Field3D &F) {
+    if (ns3d_shim_invalidate) ns3d_shim_invalidate(F);
+}
+
 extern "C" {
 
 void *ref_create(const char *solver_in) {
@@ -91,7 +105,11 @@ void *ref_create(const char *solver_in) {
     return c;
 }
 
-void ref_destroy(void *h) { delete static_cast<RefCtx *>(h); }
+void ref_destroy(void *h) {
+    auto *c = static_cast<RefCtx *>(h);
+    host_wrote(c->F);  // a later Field3D may take the same addresses
+    delete c;
+}
 
 const char *ref_last_error(void *h) { return static_cast<RefCtx *>(h)->last_error.c_str(); }
 
@@ -140,6 +158,7 @@ int ref_set_primitive(void *h, const double *rho, const double *u, const double 
         put_interior(c, c->F.p, p);
         apply_boundary(c->F, c->G, c->C, c->P);
         c->F.primitiveToConserved(c->P);
+        host_wrote(c->F);
     });
 }
 
@@ -155,12 +174,14 @@ int ref_set_conserved(void *h, const double *rho, const double *ru, const double
         c->F.conservedToPrimitive(c->P);
         apply_boundary(c->F, c->G, c->C, c->P);
         c->F.primitiveToConserved(c->P);
+        host_wrote(c->F);
     });
 }
 
 // Interior (nx*ny*nz, x fastest) of a cell-centred array.
 int ref_get(void *h, const char *name, double *out) {
     auto *c = static_cast<RefCtx *>(h);
+    host_reads(c->F);
     std::vector<double> *a = cell_field(c->F, name);
     if (!a) return -2;
     const LocalDesc &L = c->F.L;
@@ -175,6 +196,7 @@ int ref_get(void *h, const char *name, double *out) {
 // Whole ghosted array (sx*sy*sz) of a cell-centred field.
 int ref_get_full(void *h, const char *name, double *out) {
     auto *c = static_cast<RefCtx *>(h);
+    host_reads(c->F);
     std::vector<double> *a = cell_field(c->F, name);
     if (!a) return -2;
     std::memcpy(out, a->data(), a->size() * sizeof(double));
@@ -291,6 +313,7 @@ int ref_read_tecplot(void *h, const char *path, int src_nx, int src_ny, int src_
             apply_boundary(c->F, c->G, c->C, c->P);
             c->F.primitiveToConserved(c->P);
         }
+        host_wrote(c->F);
     });
     return r != 0 ? r : (ok ? 0 : 1);
 }
@@ -328,6 +351,7 @@ int ref_init_isotropic(void *h) {
         init_isotropic_turbulence(c->F, c->G, c->C, c->P);
         apply_boundary(c->F, c->G, c->C, c->P);
         c->F.primitiveToConserved(c->P);
+        host_wrote(c->F);
     });
 }
 

@@ -53,7 +53,8 @@ def isotropic_input(n: int, Ma: float = 0.5, gamma: float = 1.4) -> np.ndarray:
 def main():
     import oracle
     if not oracle.have_ref():
-        oracle.build(ref=True)
+        # this script reads the reference's own sources to make the fixtures
+        oracle.build(ref=True, ref_dir=os.environ.get("NS3D_REF_DIR") or "/root/reference")
     out = {}
     for kw in SCHEMES + CHAR_SCHEMES:
         n = 8

@@ -26,7 +26,7 @@ m = bench.dist_max(dist, 1.5 * (rank + 1), False)
 bench.run_cpu = lambda steps, warm, n: {{"value": 0.5, "cores": 1, "kind": "port",
                                         "sample": "stub", "cell_updates_per_s": 1.0}}
 class Args:
-    steps, warmup, n, gpus = 2, 3, 16, world
+    steps, warmup, n, gpus, direct_steps = 2, 3, 16, world, 0
 bench.reference_arm(Args, rank, world)
 bench.dist_barrier(dist, False)
 print(json.dumps({{"rank": rank, "world": world, "max": m}}), flush=True)
