@@ -51,6 +51,9 @@ struct ns3d_ctx {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool overlap = false;
+    // the z sweep fused with the stage update (NS3D_FUSE=1) or the two kernels
+    // (NS3D_FUSE=0); the same bits either way
+    bool fuse = false;
     long long n = 0;
     double* wmem = nullptr;      // 3 state buffers x 6 arrays x n
     int cur = 0, rec = 0;        // current state buffer, recorded (U0) buffer
@@ -525,15 +528,15 @@ ns3d_status launch_rhs_parts(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl) {
                                               : rhs_parts_t<float>(ctx, W, ctrl);
 }
 
-// One Shu-Osher stage Wc -> Wn (recorded state W0). Component-wise schemes:
-// x and y sweeps, the viscous flux, then the z sweep fused with the update
-// (k_sweep_ring<2, ..., FUSE>); characteristic-wise reconstruction: the three
-// sweeps, the viscous flux and k_update. Both give the same bits.
+// One Shu-Osher stage Wc -> Wn (recorded state W0): the three sweeps, the
+// viscous flux and k_update; or, with ctx->fuse (component-wise schemes), the
+// x and y sweeps, the viscous flux and the z sweep fused with the update
+// (k_sweep_ring<2, ..., FUSE>). Both give the same bits.
 template <class R>
 ns3d_status stage_t(ns3d_ctx* ctx, int stage, StateView Wc, StateView W0, StateOut Wn) {
     const R* tacc = (const R*)ctx->tacc;
     const R* fv = (const R*)ctx->fv;
-    if (ctx->L.chr) {
+    if (ctx->L.chr || !ctx->fuse) {
         ns3d_status s = rhs_parts_t<R>(ctx, Wc, ctx->ctrl);
         if (s != NS3D_OK) return s;
         NS3D_LAUNCH(NS3D_KERNEL_UPDATE, 1,
@@ -793,6 +796,7 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
         return bail(NS3D_ERR_CUDA, cudaGetErrorString(e));
     ctx->L.stream = ctx->stream;
     if (const char* ov = std::getenv("NS3D_OVERLAP")) ctx->overlap = std::atoi(ov) != 0;
+    if (const char* fu = std::getenv("NS3D_FUSE")) ctx->fuse = std::atoi(fu) != 0;
     if (ctx->overlap &&
         (cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
          cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||

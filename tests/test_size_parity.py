@@ -26,7 +26,12 @@ from conftest import ref_cfg, relerr
 pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
-TOL32_RHS = 5e-5
+# FP32-stencil form against the FP64 oracle on Mach_t 0.4-0.5 turbulence: the
+# mass equation's RHS is the divergence of split fluxes whose float deviations
+# (from each 64-cell segment's first cell) are O(1), so it carries ~1e-4 of its
+# maximum (measured at 256^3: WENO5 5.4e-5, UPWIND_7TH 1.2e-4; the momentum and
+# energy equations 1e-5..3e-5); two steps later the state agrees to ~2e-7
+TOL32_RHS = 3e-4
 TOL32_STATE = 1e-5
 
 
