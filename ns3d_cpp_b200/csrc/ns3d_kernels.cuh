@@ -110,9 +110,19 @@ __device__ __forceinline__ void char_face(double gamma, const double* wl, const 
 // arrays are [slot][t]: threads with consecutive t read consecutive 8- or
 // 16-byte words (no bank conflicts).
 // ---------------------------------------------------------------------------
+// Blocks per SM the ring sweeps are compiled for (register cap 65536 / (T MINB)).
+#ifndef NS3D_RING_MINB_F32
+#define NS3D_RING_MINB_F32 4
+#endif
+#ifndef NS3D_RING_MINB_F64
+#define NS3D_RING_MINB_F64 6
+#endif
+#ifndef NS3D_XW_MINB
+#define NS3D_XW_MINB 1
+#endif
 template <class R> struct RingCfg;
-template <> struct RingCfg<float> { static constexpr int T = 128, MINB = 4; };
-template <> struct RingCfg<double> { static constexpr int T = 64, MINB = 6; };
+template <> struct RingCfg<float> { static constexpr int T = 128, MINB = NS3D_RING_MINB_F32; };
+template <> struct RingCfg<double> { static constexpr int T = 64, MINB = NS3D_RING_MINB_F64; };
 
 template <class R, int S, int T> struct SplitRing;
 template <int S, int T> struct SplitRing<float, S, T> {
@@ -376,7 +386,7 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
 constexpr int XW_WARPS = 4;
 
 template <class R, int FVS, int RC, bool CHR = false>
-__global__ void __launch_bounds__(32 * XW_WARPS)
+__global__ void __launch_bounds__(32 * XW_WARPS, sizeof(R) == 4 ? NS3D_XW_MINB : 1)
 k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
     constexpr int S = Stencil<RC>::S;
@@ -742,6 +752,188 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
             for (int m = 0; m < 8; ++m) q[v2][m] = q[v2][m + 1];
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------
+// The 2.5-D viscous kernel with its plane loads pipelined (same arithmetic per
+// cell as k_visc_flux_25d, same results). Per z step:
+//   * the tile of the next plane is written into the second of two shared
+//     tiles while the current one is read, so one barrier per plane suffices;
+//   * its interior comes from the thread's own z queue (the value was loaded
+//     four planes earlier as the queue's head), only the 4-cell halo ring is
+//     loaded again (448 of 960 tile cells in the FP32 form);
+//   * the halo values and the queue head of the plane after next are copied
+//     asynchronously (cp.async, 8 bytes each) into per-thread staging slots in
+//     shared memory, so their latency hides behind a whole plane of compute
+//     and they take no registers while in flight.
+// Each thread owns its staging slots (halo cells h = tid, tid + NT, ...), so
+// the staged values need no barrier, only the thread's own wait.
+// ---------------------------------------------------------------------------
+template <class R>
+struct VPipe {
+    using T = VTile<R>;
+    static constexpr int NT = T::X * T::Y;                 // threads = interior cells
+    static constexpr int NH = T::SX * T::SY - NT;          // halo cells of a tile
+    static constexpr int HPT = (NH + NT - 1) / NT;         // halo cells per thread
+    static constexpr size_t tile_bytes = 2 * 4 * T::SY * T::SX * sizeof(R);
+    static constexpr size_t smem_bytes = tile_bytes + sizeof(double) * 4 * (NH + NT);
+    // tile coordinates (ly, lx) of halo cell h: the H top rows, the H bottom
+    // rows, then the H left and H right columns of the middle rows
+    __device__ static void halo_cell(int h, int& ly, int& lx) {
+        constexpr int H = T::H, SX = T::SX, SY = T::SY, X = T::X;
+        if (h < H * SX) {
+            ly = h / SX; lx = h - ly * SX;
+        } else if (h < 2 * H * SX) {
+            h -= H * SX; ly = SY - H + h / SX; lx = h - (h / SX) * SX;
+        } else {
+            h -= 2 * H * SX; ly = H + h / (2 * H);
+            const int c = h - (h / (2 * H)) * (2 * H);
+            lx = c < H ? c : X + c;
+        }
+    }
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <class R, int ORD>
+__global__ void __launch_bounds__(VTile<R>::X * VTile<R>::Y, 2)
+k_visc_flux_pipe(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __restrict__ ctrl,
+                 int zb) {
+    using VT = VTile<R>;
+    using VP = VPipe<R>;
+    constexpr int X = VT::X, Y = VT::Y, H = VT::H, SX = VT::SX, SY = VT::SY;
+    constexpr int NT = VP::NT, NH = VP::NH, HPT = VP::HPT;
+    if (ctrl && ctrl->stop) return;
+    constexpr bool kDeviation = sizeof(R) < sizeof(double);
+    extern __shared__ __align__(16) unsigned char vsm[];
+    R (*tile)[4][SY][SX] = reinterpret_cast<R (*)[4][SY][SX]>(vsm);          // [2][4][SY][SX]
+    double (*sth)[NH] = reinterpret_cast<double (*)[NH]>(vsm + VP::tile_bytes);  // [4][NH]
+    double (*stq)[NT] = reinterpret_cast<double (*)[NT]>(vsm + VP::tile_bytes + sizeof(double) * 4 * NH);
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = P.n, sxy = (long long)nx * ny;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * X + tx;
+    const int i0 = blockIdx.x * X, j0 = blockIdx.y * Y;
+    const int i = i0 + tx, j = j0 + ty;
+    const int k0 = blockIdx.z * zb, k1 = min(k0 + zb, nz);
+    const double* src[4] = {W.u, W.v, W.w, W.T};
+    double ref[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+        ref[v] = kDeviation ? src[v][(long long)k0 * sxy + (long long)j0 * nx + i0] : 0.0;
+    auto wrapz = [&](int k) { k %= nz; return k < 0 ? k + nz : k; };
+    // this thread's halo cells: in-plane offsets (a plane has < 2^31 cells)
+    // and flat tile positions
+    int hoff[HPT], hti[HPT];
+#pragma unroll
+    for (int c = 0; c < HPT; ++c) {
+        const int h = tid + c * NT;
+        int ly = 0, lx = 0;
+        if (h < NH) VP::halo_cell(h, ly, lx);
+        hti[c] = ly * SX + lx;
+        hoff[c] = wrap1(j0 - H + ly, ny) * nx + wrap1(i0 - H + lx, nx);
+    }
+    auto tflat = [&](int buf, int v) { return &tile[buf][v][0][0]; };
+    const long long col = (long long)j * nx + i;
+    auto issue = [&](int kh, int kq) {  // halo of plane kh, queue head of plane kq
+#pragma unroll
+        for (int c = 0; c < HPT; ++c) {
+            const int h = tid + c * NT;
+            if (h < NH) {
+                const long long off = (long long)wrapz(kh) * sxy + hoff[c];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cp_async8(&sth[v][h], src[v] + off);
+            }
+        }
+        const long long offq = (long long)wrapz(kq) * sxy + col;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) cp_async8(&stq[v][tid], src[v] + offq);
+        cp_async_commit();
+    };
+    // prologue: queue planes k0-4 .. k0+3, tile 0 = plane k0, staging = (halo k0+1, head k0+4)
+    R q[4][9];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const long long off = (long long)wrapz(k0 - 4 + m) * sxy + col;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[v][m] = R(src[v][off] - ref[v]);
+    }
+#pragma unroll
+    for (int c = 0; c < HPT; ++c) {
+        const int h = tid + c * NT;
+        if (h < NH) {
+            const long long off = (long long)k0 * sxy + hoff[c];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) tflat(0, v)[hti[c]] = R(src[v][off] - ref[v]);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) tile[0][v][ty + H][tx + H] = q[v][4];
+    issue(k0 + 1, k0 + 4);
+    __syncthreads();
+    const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
+    const R mu_ref = R(P.mu), Ss = R(P.sutherland_s), Cp = R(P.Cp), Pr = R(P.Pr);
+    int b = 0;
+    for (int k = k0; k < k1; ++k) {
+        // the staged halo of plane k+1 and head of plane k+4 (this thread's own copies)
+        cp_async_wait_all();
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[v][8] = R(stq[v][tid] - ref[v]);
+        if (k + 1 < k1) {
+            // tile of plane k+1 into the other buffer (everyone finished reading it)
+#pragma unroll
+            for (int c = 0; c < HPT; ++c) {
+                const int h = tid + c * NT;
+                if (h < NH) {
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) tflat(b ^ 1, v)[hti[c]] = R(sth[v][h] - ref[v]);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) tile[b ^ 1][v][ty + H][tx + H] = q[v][5];
+            issue(k + 2, k + 5);
+        }
+        const int cx = tx + H, cy = ty + H;
+        R g[4][3];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            g[v][0] = dcentral<R, ORD>([&](int o) { return tile[b][v][cy][cx + o]; }, dx);
+            g[v][1] = dcentral<R, ORD>([&](int o) { return tile[b][v][cy + o][cx]; }, dy);
+            g[v][2] = dcentral<R, ORD>([&](int o) { return q[v][4 + o]; }, dz);
+        }
+        const R du_dx = g[0][0], du_dy = g[0][1], du_dz = g[0][2];
+        const R dv_dx = g[1][0], dv_dy = g[1][1], dv_dz = g[1][2];
+        const R dw_dx = g[2][0], dw_dy = g[2][1], dw_dz = g[2][2];
+        const R dT_dx = g[3][0], dT_dy = g[3][1], dT_dz = g[3][2];
+        const R mu = get_mu<R>(R(ref[3]) + q[3][4], mu_ref, Ss);
+        const R divU = du_dx + dv_dy + dw_dz;
+        const R tau_xx = R(2.0) * mu * du_dx - R(2.0 / 3.0) * mu * divU;
+        const R tau_yy = R(2.0) * mu * dv_dy - R(2.0 / 3.0) * mu * divU;
+        const R tau_zz = R(2.0) * mu * dw_dz - R(2.0 / 3.0) * mu * divU;
+        const R tau_xy = mu * (du_dy + dv_dx);
+        const R tau_xz = mu * (du_dz + dw_dx);
+        const R tau_yz = mu * (dv_dz + dw_dy);
+        const R qx = mu * Cp / Pr * dT_dx;
+        const R qy = mu * Cp / Pr * dT_dy;
+        const R qz = mu * Cp / Pr * dT_dz;
+        const R u = R(ref[0]) + q[0][4], v = R(ref[1]) + q[1][4], w = R(ref[2]) + q[2][4];
+        const long long id = (long long)k * sxy + col;
+        store_fv<R>(fv, n, id, tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz,
+                    u * tau_xx + v * tau_xy + w * tau_xz + qx,
+                    u * tau_xy + v * tau_yy + w * tau_yz + qy,
+                    u * tau_xz + v * tau_yz + w * tau_zz + qz);
+#pragma unroll
+        for (int v2 = 0; v2 < 4; ++v2)
+#pragma unroll
+            for (int m = 0; m < 8; ++m) q[v2][m] = q[v2][m + 1];
+        b ^= 1;
+        __syncthreads();
+    }
+    cp_async_wait_all();
 }
 
 // Viscous part of the rhs at one cell: compute_vis_flux (ViscousFlux.cpp:370-384,

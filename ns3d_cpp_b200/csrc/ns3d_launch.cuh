@@ -191,6 +191,27 @@ inline dim3 grid_25d(const LaunchCfg& L) {
 
 template <class R>
 cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl) {
+    if (detail::tiles_25d<R>(L, 1) && (L.tiled & 2)) {
+        const dim3 g = detail::grid_25d<R>(L), b(VTile<R>::X, VTile<R>::Y);
+        const int zb = detail::zb_for<R>(L);
+        constexpr int sm = (int)VPipe<R>::smem_bytes;
+        auto go = [&](auto kern) -> cudaError_t {
+            static bool attr = false;  // opt in to > 48 KB of dynamic shared memory once
+            if (!attr) {
+                const cudaError_t e =
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+                if (e != cudaSuccess) return e;
+                attr = true;
+            }
+            kern<<<g, b, sm, L.stream>>>(L.P, W, fv, ctrl, zb);
+            return cudaGetLastError();
+        };
+        switch (L.P.vis_order) {
+        case 4: return go(k_visc_flux_pipe<R, 4>);
+        case 6: return go(k_visc_flux_pipe<R, 6>);
+        default: return go(k_visc_flux_pipe<R, 8>);
+        }
+    }
     if (detail::tiles_25d<R>(L, 1)) {
         const dim3 g = detail::grid_25d<R>(L), b(VTile<R>::X, VTile<R>::Y);
         switch (L.P.vis_order) {
