@@ -12,6 +12,7 @@
 #include <cstring>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <thread>
 #include <vector>
 
@@ -137,9 +138,26 @@ ns3d_status launch(ns3d_ctx* ctx, int cls, int nk, F&& f) {
     return launch_on(ctx, ctx->stream, cls, nk, f);
 }
 
+// The status of `expr`: a launcher's own cudaError_t (an attribute or
+// configuration failure it returns) or, for raw <<<>>> launches (void), the
+// launch error.
+template <class F>
+cudaError_t launch_result(F&& f) {
+    if constexpr (std::is_void_v<decltype(f())>) {
+        f();
+        return cudaGetLastError();
+    } else {
+        const cudaError_t e = f();
+        const cudaError_t e2 = cudaGetLastError();
+        return e != cudaSuccess ? e : e2;
+    }
+}
+
 #define NS3D_LAUNCH(cls, nk, expr)                                                   \
     do {                                                                             \
-        ns3d_status s_ = launch(ctx, (cls), (nk), [&]() -> cudaError_t { expr; return cudaGetLastError(); }); \
+        ns3d_status s_ = launch(ctx, (cls), (nk), [&]() -> cudaError_t {             \
+            return launch_result([&]() { return expr; });                            \
+        });                                                                          \
         if (s_ != NS3D_OK) return s_;                                                \
     } while (0)
 
@@ -506,8 +524,7 @@ ns3d_status rhs_parts_t(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl, int dirs =
         LaunchCfg Ls = ctx->L;
         Ls.stream = ctx->side;
         ns3d_status s = launch_on(ctx, ctx->side, NS3D_KERNEL_VISC_FLUX, 1, [&]() -> cudaError_t {
-            launch_visc_flux<R>(Ls, W, (R*)ctx->fv, ctrl);
-            return cudaGetLastError();
+            return launch_result([&]() { return launch_visc_flux<R>(Ls, W, (R*)ctx->fv, ctrl); });
         });
         if (s != NS3D_OK) return s;
         NS3D_CK(cudaEventRecord(ctx->ev_join, ctx->side));
@@ -701,7 +718,7 @@ namespace ns3d {
 // fewer planes per block (detail::zb_for) so that the grid fills the SMs.
 void default_tiling(LaunchCfg& L) {
     L.zb = 0;
-    L.tiled = 1;
+    L.tiled = 3;  // 2.5-D viscous flux, pipelined plane loads (k_visc_flux_pipe)
     if (const char* e = std::getenv("NS3D_TILE_ZB")) L.zb = std::atoi(e);
     if (const char* e = std::getenv("NS3D_TILED")) L.tiled = std::atoi(e);
     if (const char* e = std::getenv("NS3D_SEG"))

@@ -19,7 +19,7 @@ struct LaunchCfg {
     int seg[3];   // cells per thread segment along x, y, z
     cudaStream_t stream;
     int zb;       // planes per block of the 2.5-D viscous kernels (0: from the grid)
-    int tiled;    // bit 0: 2.5-D visc_flux (when the box tiles)
+    int tiled;    // bit 0: 2.5-D visc_flux (when the box tiles); bit 1: its pipelined form
 };
 
 // Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED / NS3D_SEG for tuning.
@@ -187,29 +187,34 @@ inline dim3 grid_25d(const LaunchCfg& L) {
     const int zb = zb_for<R>(L);
     return dim3(L.P.nx / VTile<R>::X, L.P.ny / VTile<R>::Y, (L.P.nz + zb - 1) / zb);
 }
+// k_visc_flux_pipe<R, ORD>: more than 48 KB of dynamic shared memory, opted
+// in once per instantiation and device (setting it twice is harmless).
+template <class R, int ORD>
+cudaError_t visc_pipe(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl) {
+    constexpr int sm = (int)VPipe<R>::smem_bytes;
+    static bool opted[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !opted[dev]) {
+        e = cudaFuncSetAttribute(k_visc_flux_pipe<R, ORD>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) opted[dev] = true;
+    }
+    const dim3 g = grid_25d<R>(L), b(VTile<R>::X, VTile<R>::Y);
+    k_visc_flux_pipe<R, ORD><<<g, b, sm, L.stream>>>(L.P, W, fv, ctrl, zb_for<R>(L));
+    return cudaGetLastError();
+}
 }  // namespace detail
 
 template <class R>
 cudaError_t launch_visc_flux(const LaunchCfg& L, StateView W, R* fv, const Ctrl* ctrl) {
     if (detail::tiles_25d<R>(L, 1) && (L.tiled & 2)) {
-        const dim3 g = detail::grid_25d<R>(L), b(VTile<R>::X, VTile<R>::Y);
-        const int zb = detail::zb_for<R>(L);
-        constexpr int sm = (int)VPipe<R>::smem_bytes;
-        auto go = [&](auto kern) -> cudaError_t {
-            static bool attr = false;  // opt in to > 48 KB of dynamic shared memory once
-            if (!attr) {
-                const cudaError_t e =
-                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-                if (e != cudaSuccess) return e;
-                attr = true;
-            }
-            kern<<<g, b, sm, L.stream>>>(L.P, W, fv, ctrl, zb);
-            return cudaGetLastError();
-        };
         switch (L.P.vis_order) {
-        case 4: return go(k_visc_flux_pipe<R, 4>);
-        case 6: return go(k_visc_flux_pipe<R, 6>);
-        default: return go(k_visc_flux_pipe<R, 8>);
+        case 4: return detail::visc_pipe<R, 4>(L, W, fv, ctrl);
+        case 6: return detail::visc_pipe<R, 6>(L, W, fv, ctrl);
+        default: return detail::visc_pipe<R, 8>(L, W, fv, ctrl);
         }
     }
     if (detail::tiles_25d<R>(L, 1)) {
