@@ -117,9 +117,6 @@ __device__ __forceinline__ void char_face(double gamma, const double* wl, const 
 #ifndef NS3D_RING_MINB_F64
 #define NS3D_RING_MINB_F64 6
 #endif
-#ifndef NS3D_XW_MINB
-#define NS3D_XW_MINB 1
-#endif
 template <class R> struct RingCfg;
 template <> struct RingCfg<float> { static constexpr int T = 128, MINB = NS3D_RING_MINB_F32; };
 template <> struct RingCfg<double> { static constexpr int T = 64, MINB = NS3D_RING_MINB_F64; };
@@ -386,7 +383,7 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
 constexpr int XW_WARPS = 4;
 
 template <class R, int FVS, int RC, bool CHR = false>
-__global__ void __launch_bounds__(32 * XW_WARPS, sizeof(R) == 4 ? NS3D_XW_MINB : 1)
+__global__ void __launch_bounds__(32 * XW_WARPS)
 k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
     constexpr int S = Stencil<RC>::S;
