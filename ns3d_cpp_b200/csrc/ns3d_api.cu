@@ -46,15 +46,12 @@ struct ns3d_ctx {
     LaunchCfg L;
     int device = 0;
     cudaStream_t stream = nullptr;
-    // The RHS pieces of a stage run concurrently: the x sweep on `stream`, the
-    // y and z sweeps and the viscous flux on three side streams (each sweep
-    // writes its own accumulator block, tsep > 0), joined before the update.
-    // They fill each other's last waves (the y / z sweeps are 3.5 waves of
-    // blocks at 256^3) and mix the issue-bound sweeps with the latency-bound
-    // viscous kernel. NS3D_CONCURRENT=0 runs them one after the other.
-    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
-    bool concurrent = true;
+    // the viscous flux can run beside the sweeps on a second stream (NS3D_OVERLAP=1;
+    // measured at 256^3 FP32: 8.13 -> 8.04 ms per step, the sweep it shares the
+    // SMs with stretching by about the viscous kernel's time, so it is off by default)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool overlap = false;
     // the z sweep fused with the stage update (NS3D_FUSE=1) or the two kernels
     // (NS3D_FUSE=0); the same bits either way
     bool fuse = false;
@@ -515,49 +512,30 @@ ns3d_status read_ctrl(ns3d_ctx* ctx) {
 
 // The RHS pieces of the current state into tacc/fv: the sweeps along x, y and
 // (unless `dirs` is 2, when the z sweep is left to the fused stage kernel) z,
-// and the viscous flux. With per-direction accumulator blocks and
-// ctx->concurrent the pieces run on four streams (x on the context's stream);
-// with the chained block only the viscous flux runs beside the sweeps.
+// and the viscous flux.
 template <class R>
 ns3d_status rhs_parts_t(ns3d_ctx* ctx, StateView W, const Ctrl* ctrl, int dirs = 3) {
     R* tacc = (R*)ctx->tacc;
-    if (!ctx->concurrent) {
+    if (ctx->overlap) {
+        // the viscous flux (state -> fv) beside the sweeps (state -> T_acc):
+        // fork after the work already queued, join before the update
+        NS3D_CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+        NS3D_CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+        LaunchCfg Ls = ctx->L;
+        Ls.stream = ctx->side;
+        ns3d_status s = launch_on(ctx, ctx->side, NS3D_KERNEL_VISC_FLUX, 1, [&]() -> cudaError_t {
+            return launch_result([&]() { return launch_visc_flux<R>(Ls, W, (R*)ctx->fv, ctrl); });
+        });
+        if (s != NS3D_OK) return s;
+        NS3D_CK(cudaEventRecord(ctx->ev_join, ctx->side));
         for (int dir = 0; dir < dirs; ++dir)
             NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X + dir, 1, launch_sweep<R>(ctx->L, dir, W, tacc, ctrl));
-        NS3D_LAUNCH(NS3D_KERNEL_VISC_FLUX, 1, launch_visc_flux<R>(ctx->L, W, (R*)ctx->fv, ctrl));
+        NS3D_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
         return NS3D_OK;
     }
-    const bool split = ctx->L.P.tsep > 0;
-    // fork after the work already queued on the context's stream
-    NS3D_CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
-    for (int k = 0; k < 3; ++k) NS3D_CK(cudaStreamWaitEvent(ctx->side[k], ctx->ev_fork, 0));
-    auto on = [&](int k, int cls, auto&& f) -> ns3d_status {
-        LaunchCfg Ls = ctx->L;
-        Ls.stream = ctx->side[k];
-        return launch_on(ctx, ctx->side[k], cls, 1, [&]() -> cudaError_t {
-            return launch_result([&]() { return f(Ls); });
-        });
-    };
-    ns3d_status s = on(0, NS3D_KERNEL_VISC_FLUX, [&](const LaunchCfg& Ls) {
-        return launch_visc_flux<R>(Ls, W, (R*)ctx->fv, ctrl);
-    });
-    if (s != NS3D_OK) return s;
-    if (split) {
-        for (int dir = 1; dir < dirs; ++dir) {
-            s = on(dir, NS3D_KERNEL_SWEEP_X + dir, [&](const LaunchCfg& Ls) {
-                return launch_sweep<R>(Ls, dir, W, tacc, ctrl);
-            });
-            if (s != NS3D_OK) return s;
-        }
-        NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X, 1, launch_sweep<R>(ctx->L, 0, W, tacc, ctrl));
-    } else {
-        for (int dir = 0; dir < dirs; ++dir)
-            NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X + dir, 1, launch_sweep<R>(ctx->L, dir, W, tacc, ctrl));
-    }
-    for (int k = 0; k < 3; ++k) {
-        NS3D_CK(cudaEventRecord(ctx->ev_join[k], ctx->side[k]));
-        NS3D_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join[k], 0));
-    }
+    for (int dir = 0; dir < dirs; ++dir)
+        NS3D_LAUNCH(NS3D_KERNEL_SWEEP_X + dir, 1, launch_sweep<R>(ctx->L, dir, W, tacc, ctrl));
+    NS3D_LAUNCH(NS3D_KERNEL_VISC_FLUX, 1, launch_visc_flux<R>(ctx->L, W, (R*)ctx->fv, ctrl));
     return NS3D_OK;
 }
 
@@ -834,21 +812,16 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(NS3D_ERR_CUDA, cudaGetErrorString(e));
     ctx->L.stream = ctx->stream;
-    if (const char* cc = std::getenv("NS3D_CONCURRENT")) ctx->concurrent = std::atoi(cc) != 0;
+    if (const char* ov = std::getenv("NS3D_OVERLAP")) ctx->overlap = std::atoi(ov) != 0;
     if (const char* fu = std::getenv("NS3D_FUSE")) ctx->fuse = std::atoi(fu) != 0;
-    if (ctx->concurrent) {
-        bool ok = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) == cudaSuccess;
-        for (int k = 0; k < 3 && ok; ++k)
-            ok = cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking) == cudaSuccess &&
-                 cudaEventCreateWithFlags(&ctx->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
-        if (!ok) return bail(NS3D_ERR_CUDA, "side streams for the concurrent RHS pieces");
-    }
+    if (ctx->overlap &&
+        (cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+         cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+         cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess))
+        return bail(NS3D_ERR_CUDA, "second stream for the overlapped viscous flux");
     const size_t n = (size_t)ctx->n;
-    // one accumulator block per direction (the sweeps independent of each
-    // other), except for the fused z sweep, which adds to the x + y terms
-    ctx->L.P.tsep = ctx->fuse ? 0 : 5 * ctx->n;
     if (cudaMalloc(&ctx->wmem, sizeof(double) * 18 * n) != cudaSuccess ||
-        cudaMalloc(&ctx->tacc, ctx->rsize * (ctx->fuse ? 5 : 15) * n) != cudaSuccess ||
+        cudaMalloc(&ctx->tacc, ctx->rsize * 5 * n) != cudaSuccess ||
         cudaMalloc(&ctx->fv, ctx->rsize * (ctx->rsize == 4 ? fv_values_per_cell<float>() : fv_values_per_cell<double>()) * n) != cudaSuccess ||
         cudaMalloc(&ctx->ctrl, sizeof(Ctrl)) != cudaSuccess) {
         cudaGetLastError();
@@ -886,10 +859,8 @@ ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
     if (ctx->ctrl_host) cudaFreeHost(ctx->ctrl_host);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-    for (int k = 0; k < 3; ++k) {
-        if (ctx->ev_join[k]) cudaEventDestroy(ctx->ev_join[k]);
-        if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
-    }
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NS3D_OK;

@@ -36,11 +36,6 @@ struct DevParams {
     double lin[8];   // linear reconstruction coefficients (LIN6 / LIN8)
     double mdcd_disp, mdcd_diss;
     int vis_order;   // 4, 6, 8
-    // inviscid accumulator layout: 0 -- one 5n block, the y and z sweeps add to
-    // the x term in place (T = (ax idx + ay idy) + az idz); 5n -- one block per
-    // direction (x, y, z at offsets 0, tsep, 2 tsep), summed in that order by
-    // the reader, so the three sweeps are independent of each other
-    long long tsep;
 };
 
 // ---------------------------------------------------------------------------

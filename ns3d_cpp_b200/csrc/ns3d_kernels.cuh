@@ -230,7 +230,6 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
     const int c0 = blockIdx.z * seg;
     if (c0 >= len) return;
     const int c1 = min(c0 + seg, len);
-    R* __restrict__ tout = tacc + DIR * P.tsep;  // this direction's block (chained: the one block)
 
     const R gamma = R(P.gamma), eps = R(P.sw_eps);
     R lin[8];
@@ -318,10 +317,10 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
         for (int q = 0; q < 5; ++q) cur[q] = nxt[q];
         // the following cell (in range by wrap-around even past the segment end)
         load_raw(f - MID + S, nxt);
-        R old[5] = {R(0), R(0), R(0), R(0), R(0)};
+        R old[5];
         const long long oid = base + (long long)f * stride;
         if constexpr (DIR != 0) {
-            if (t > 0 && P.tsep == 0) {
+            if (t > 0) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) old[q] = tacc[q * n + oid];
             }
@@ -352,10 +351,10 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 const R d = face[q] - prev[q];
-                if (DIR == 0 || P.tsep > 0)
-                    tout[q * n + oid] = d * inv_h;
+                if constexpr (DIR == 0)
+                    tacc[q * n + oid] = d * inv_h;
                 else
-                    tout[q * n + oid] = old[q] + d * inv_h;
+                    tacc[q * n + oid] = old[q] + d * inv_h;
             }
         }
 #pragma unroll
@@ -999,16 +998,8 @@ __device__ __forceinline__ void cell_rhs(const DevParams& P, const R* __restrict
                                          long long id, R r[5]) {
     cell_visc<R, ORD>(P, fv, i, j, k, id, r);
     const long long n = P.n;
-    if (P.tsep == 0) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) r[q] += -tacc[q * n + id];
-    } else {
-        // ((ax idx + ay idy) + az idz), the reference's order (range_kutta.cpp:61-97)
-        const long long t = P.tsep;
-#pragma unroll
-        for (int q = 0; q < 5; ++q)
-            r[q] += -((tacc[q * n + id] + tacc[t + q * n + id]) + tacc[2 * t + q * n + id]);
-    }
+    for (int q = 0; q < 5; ++q) r[q] += -tacc[q * n + id];
 }
 
 // compute_rhs output (5 blocks of n, double).
@@ -1341,8 +1332,8 @@ k_sweep_ring(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl
             for (int q = 0; q < 5; ++q) cur[q] = nxt[q];
             load_raw(f - MID + S, nxt);  // the following cell, one step ahead
             const long long oid = base + (long long)f * stride;
-            R old[5] = {R(0), R(0), R(0), R(0), R(0)};
-            if (t > 0 && (FUSE || P.tsep == 0)) {
+            R old[5];
+            if (t > 0) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) old[q] = tacc[q * n + oid];
             }
@@ -1379,18 +1370,15 @@ k_sweep_ring(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl
             if (t > 0) {
                 R tz[5];
 #pragma unroll
-                for (int q = 0; q < 5; ++q)
-                    tz[q] = (FUSE || P.tsep == 0) ? old[q] + (face[q] - prev[q]) * inv_h
-                                                  : (face[q] - prev[q]) * inv_h;
+                for (int q = 0; q < 5; ++q) tz[q] = old[q] + (face[q] - prev[q]) * inv_h;
                 if constexpr (FUSE) {
                     const int i = t0, j = blockIdx.y;
                     if (F.stage == 1) fused_cell<R, 1>(P, W, F, i, j, f, oid, tz, dt, cand);
                     else if (F.stage == 2) fused_cell<R, 2>(P, W, F, i, j, f, oid, tz, dt, cand);
                     else fused_cell<R, 3>(P, W, F, i, j, f, oid, tz, dt, cand);
                 } else {
-                    R* __restrict__ tout = tacc + DIR * P.tsep;
 #pragma unroll
-                    for (int q = 0; q < 5; ++q) tout[q * n + oid] = tz[q];
+                    for (int q = 0; q < 5; ++q) tacc[q * n + oid] = tz[q];
                 }
             }
 #pragma unroll
