@@ -189,6 +189,11 @@ ns3d_status ns3d_time_advance_segment(ns3d_ctx *ctx, int max_steps, double *time
                                       int *events);
 /* dt of the last step taken on the device. */
 ns3d_status ns3d_last_dt(ns3d_ctx *ctx, double *dt);
+/* current_time after each step the last ns3d_step / ns3d_time_advance /
+ * ns3d_time_advance_segment call completed (the value the reference prints in
+ * its "Completed step" line, maincycle.cpp:56-58): copies up to `cap` of them
+ * to `times` (may be NULL with cap 0) and stores their number in *n. */
+ns3d_status ns3d_step_times(ns3d_ctx *ctx, double *times, int cap, int *n);
 
 /* ---- discrete adjoint (no counterpart in the reference) ------------------- */
 /* The derivative of exactly the FP64 forward arithmetic (the adjoint of the

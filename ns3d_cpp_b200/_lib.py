@@ -48,6 +48,7 @@ _SIGS = {
     "ns3d_time_advance": (_i, [_vp, _i, _D, ctypes.POINTER(ctypes.c_int)]),
     "ns3d_step": (_i, [_vp, _i]),
     "ns3d_last_dt": (_i, [_vp, _D]),
+    "ns3d_step_times": (_i, [_vp, _D, _i, ctypes.POINTER(ctypes.c_int)]),
     "ns3d_total_energy": (_i, [_vp, _D]),
     "ns3d_energy_spectrum": (_i, [_vp, _D, _i]),
     "ns3d_turbulence_stats": (_i, [_vp, _vp]),

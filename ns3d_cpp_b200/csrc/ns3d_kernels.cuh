@@ -382,19 +382,32 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
 // ---------------------------------------------------------------------------
 constexpr int XW_WARPS = 4;
 
+template <class R, int FVS, int RC, bool CHR>
+__device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView& W,
+                                            R* __restrict__ tacc, SplitRing<R, XW_WARPS, 96>& ring,
+                                            int wq, int lane, long long row);
+
 template <class R, int FVS, int RC, bool CHR = false>
 __global__ void __launch_bounds__(32 * XW_WARPS)
 k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
+    __shared__ SplitRing<R, XW_WARPS, 96> ring;  // [warp][3 chunks x 32 cells]
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const long long row = (long long)blockIdx.x * XW_WARPS + wq;
+    if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
+    x_sweep_row<R, FVS, RC, CHR>(P, W, tacc, ring, wq, lane, row);
+}
+
+// The x sweep of one periodic row by one warp (the body of k_sweep_x_warp).
+template <class R, int FVS, int RC, bool CHR>
+__device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView& W,
+                                            R* __restrict__ tacc, SplitRing<R, XW_WARPS, 96>& ring,
+                                            int wq, int lane, long long row) {
     constexpr int S = Stencil<RC>::S;
     constexpr int MID = (S - 1) / 2;
     constexpr bool kDeviation = sizeof(R) < sizeof(double);
-    __shared__ SplitRing<R, XW_WARPS, 96> ring;  // [warp][3 chunks x 32 cells]
-    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
     const int nx = P.nx;
     const long long n = P.n;
-    const long long row = (long long)blockIdx.x * XW_WARPS + wq;
-    if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
     const long long base = row * nx;
     const int nch = nx >> 5;
     const R gamma = R(P.gamma), eps = R(P.sw_eps);
@@ -1455,7 +1468,8 @@ __global__ void k_control_pre(Ctrl* c, int mode, double cfl, double dt_fixed, do
 }
 
 // End of one iteration (maincycle.cpp:250 + 298-300, range_kutta.cpp:149-162).
-__global__ void k_control_post(Ctrl* c, int mode, double total_time, long long n) {
+__global__ void k_control_post(Ctrl* c, int mode, double total_time, long long n,
+                               double* times) {
     if (c->stop || !c->active) return;
     c->active = 0;
     c->steps_done += 1;
@@ -1464,6 +1478,7 @@ __global__ void k_control_post(Ctrl* c, int mode, double total_time, long long n
         c->stop_reason = STOP_NONPHYSICAL;
         return;
     }
+    times[c->steps_done - 1] = c->time;  // current_time after the step
     if (mode >= 1 && c->time >= total_time) {
         c->stop = 1;
         c->stop_reason = STOP_TOTAL_TIME;

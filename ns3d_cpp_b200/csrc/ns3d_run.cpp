@@ -8,6 +8,8 @@
 // waits where the reference writes something. What the reference writes there,
 // and in which order, is reproduced:
 //
+//   every step: "Completed step n / max, Time = t / TotalTime" (verbose), from
+//     the times the device recorded during the segment (ns3d_step_times)
 //   monitor step (step == 1 or step % monitor_Stepfreq == 0):
 //     compute_diagnostics           -> ns3d_residuals          (monitor_res)
 //     compute_total_energy          -> ns3d_total_energy       (monitor_energy)
@@ -21,6 +23,10 @@
 //
 // The statistics row takes the spectrum as the reference does: rounded to the
 // 6 digits of its spectrum file and read back (ana_isotropic.cpp:210-221).
+//
+// The reference's stdout switches to std::fixed with 6 decimals at its first
+// "[Step" line and stays there, so the times of the lines printed before it
+// (the first "Completed step" line) appear in the stream's default %g form.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -41,6 +47,27 @@ struct Monitor {
     std::string out;            // <workdir>/output
     double etot = 0.0;          // F.global_Etot: the last computed total energy
     double res[5] = {0, 0, 0, 0, 0};
+    bool fixed = false;         // stdout in std::fixed, setprecision(6)
+
+    // a time as the reference's stdout formats it at this point
+    const char* fmt_time(double v, char* buf, size_t n) const {
+        std::snprintf(buf, n, fixed ? "%.6f" : "%g", v);
+        return buf;
+    }
+
+    // "Completed step" lines (maincycle.cpp:56-58) of the `done` steps ending
+    // at step `last`
+    ns3d_status completed(int last, int done, int max_steps) {
+        std::vector<double> times(done);
+        int got = 0;
+        ns3d_status s = ns3d_step_times(ctx, times.data(), done, &got);
+        if (s != NS3D_OK) return s;
+        char a[64], b[64];
+        for (int k = 0; k < std::min(got, done); ++k)
+            std::printf("Completed step %d / %d, Time = %s / %s\n", last - done + 1 + k, max_steps,
+                        fmt_time(times[k], a, sizeof a), fmt_time(p.TotalTime, b, sizeof b));
+        return NS3D_OK;
+    }
 
     // isotropic_post_process (postprocess.cpp:133-145) at time t
     ns3d_status isotropic(double t) {
@@ -74,6 +101,7 @@ struct Monitor {
             if (p.monitor_energy) std::printf("  Ek_avg=%.6f", etot);
             std::printf("\n");
             std::fflush(stdout);
+            fixed = true;
         }
         if (p.monitor_res &&
             (s = ns3d_residuals_write((out + "/output_residuals.dat").c_str(), step, res, etot)) !=
@@ -125,6 +153,10 @@ extern "C" ns3d_status ns3d_run(ns3d_ctx* ctx, const char* workdir, int max_step
         int done = 0, events = 0;
         s = ns3d_time_advance_segment(ctx, n, &t, &done, &events);
         step += done;
+        if (verbose && done > 0) {
+            const ns3d_status sc = m.completed(step, done, max_steps);
+            if (s == NS3D_OK) s = sc;
+        }
         if (s != NS3D_OK || done == 0) break;
         if (step == 1 || step % m.p.monitor_Stepfreq == 0) {
             const Clock::time_point now = Clock::now();
@@ -136,9 +168,13 @@ extern "C" ns3d_status ns3d_run(ns3d_ctx* ctx, const char* workdir, int max_step
         if ((events & NS3D_EVENT_OUTPUT) && (s = m.output(t)) != NS3D_OK) break;
         if (events & NS3D_EVENT_END) break;
     }
-    if (verbose)
-        std::printf("Simulation complete. Total time: %g s\n",
-                    std::chrono::duration<double>(Clock::now() - t_start).count());
+    if (verbose) {
+        char a[64];
+        std::printf("Simulation complete. Total time: %s s\n",
+                    m.fmt_time(std::chrono::duration<double>(Clock::now() - t_start).count(), a,
+                               sizeof a));
+        std::fflush(stdout);
+    }
     if (time) *time = t;
     if (steps_done) *steps_done = step - (int)done0;
     return s;

@@ -260,6 +260,17 @@ class Solver:
         self._ck(self.lib.ns3d_last_dt(self.ctx, ctypes.byref(dt)))
         return dt.value
 
+    def step_times(self) -> np.ndarray:
+        """current_time after each step of the last step / time_advance call."""
+        n = ctypes.c_int()
+        self._ck(self.lib.ns3d_step_times(self.ctx, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value)
+        if n.value:
+            self._ck(self.lib.ns3d_step_times(
+                self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n.value,
+                ctypes.byref(n)))
+        return out
+
     def synchronize(self) -> None:
         self._ck(self.lib.ns3d_synchronize(self.ctx))
 

@@ -95,11 +95,16 @@ def test_time_advance_clipping_matches_oracle(oracle_mod):
     with ns.Solver(params_from_cfg(cfg)) as s:
         s.upload_primitive(W)
         tg, kg = s.time_advance(40)
+        times = s.step_times()
         Wg = s.download_primitive()
         # already at TotalTime: a further call takes no step
         tg2, kg2 = s.time_advance(5)
+        assert len(s.step_times()) == 0
     assert kg == steps and abs(tg - t) <= 1e-15
     assert kg2 == 0 and tg2 == tg
+    # current_time after every step, as the reference's "Completed step" line has it
+    assert len(times) == steps and times[-1] == tg
+    assert np.allclose(times, np.cumsum(dts), rtol=1e-14, atol=0)
     assert np.all(relerr(Wg, W2) <= TOL64)
 
 

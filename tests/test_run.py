@@ -8,6 +8,7 @@ files as the reference's own time_advance, with the same values to the digits
 printed."""
 import ctypes
 import os
+import re
 import tempfile
 
 import numpy as np
@@ -175,6 +176,59 @@ def test_run_writes_the_reference_files(oracle_mod, kw):
         assert abs(t - 0.3) < 1e-12 and k < 20
     else:
         assert k == 9
+
+
+def _stdout_lines(text):
+    """The "Completed step" and "[Step" lines, wall-clock fields removed."""
+    out = []
+    for line in text.splitlines():
+        if line.startswith("Completed step"):
+            out.append(line)
+        elif line.startswith("[Step"):
+            out.append(re.sub(r"Time/step=\S+s  Elapsed=\S+s", "", line))
+    return out
+
+
+@needs_ref
+@pytest.mark.gpu
+def test_run_prints_the_reference_step_lines(oracle_mod, capfd):
+    """ns3d_run's stdout against the reference's own time_advance
+    (maincycle.cpp:56-86): one "Completed step" line per step with the same
+    step numbers and times, the monitor lines in the same places, the same
+    number formats (the stream turns to fixed 6 decimals at the first monitor
+    line). The first line's time is compared by value: an earlier reference
+    run in this process may have left its stream in fixed format."""
+    n = 16
+    cfg = run_cfg(n, TotalTime=0.3, monitor_Stepfreq=3, max_steps=20)
+    W = tgv(n, seed=5)
+    libc = ctypes.CDLL(None)
+    r = oracle_mod.Ref(cfg)
+    r.set_primitive(W)
+    with tempfile.TemporaryDirectory() as d:
+        dr, dg = os.path.join(d, "ref"), os.path.join(d, "gpu")
+        os.makedirs(dr)
+        libc.fflush(None)
+        capfd.readouterr()
+        r.time_advance(dr)
+        libc.fflush(None)
+        ref_out = capfd.readouterr().out
+        with ns.Solver(params_for(cfg)) as s:
+            s.upload_primitive(W)
+            t, k = s.run(dg, verbose=True)
+            times = s.step_times()
+        libc.fflush(None)
+        gpu_out = capfd.readouterr().out
+    a, b = _stdout_lines(ref_out), _stdout_lines(gpu_out)
+    assert sum(x.startswith("Completed") for x in a) == k > 3
+    assert len(a) == len(b)
+    head_a, head_b = a[0].split("Time = "), b[0].split("Time = ")
+    assert head_a[0] == head_b[0]
+    assert float(head_a[1].split(" / ")[0]) == pytest.approx(float(head_b[1].split(" / ")[0]),
+                                                            rel=1e-6)
+    assert a[1:] == b[1:]
+    assert "Simulation complete. Total time: " in gpu_out
+    # the record of the last segment ends at the returned time
+    assert len(times) >= 1 and times[-1] == t
 
 
 @pytest.mark.gpu
