@@ -117,8 +117,11 @@ __device__ __forceinline__ void char_face(double gamma, const double* wl, const 
 #ifndef NS3D_RING_MINB_F64
 #define NS3D_RING_MINB_F64 6
 #endif
+#ifndef NS3D_RING_T_F32
+#define NS3D_RING_T_F32 128
+#endif
 template <class R> struct RingCfg;
-template <> struct RingCfg<float> { static constexpr int T = 128, MINB = NS3D_RING_MINB_F32; };
+template <> struct RingCfg<float> { static constexpr int T = NS3D_RING_T_F32, MINB = NS3D_RING_MINB_F32; };
 template <> struct RingCfg<double> { static constexpr int T = 64, MINB = NS3D_RING_MINB_F64; };
 
 template <class R, int S, int T> struct SplitRing;
@@ -380,7 +383,10 @@ k_sweep(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __r
 // k_sweep<0> (the FP64 results are identical); in the FP32-stencil form the
 // split-flux offset is the row's first cell.
 // ---------------------------------------------------------------------------
-constexpr int XW_WARPS = 4;
+#ifndef NS3D_XW_WARPS
+#define NS3D_XW_WARPS 4
+#endif
+constexpr int XW_WARPS = NS3D_XW_WARPS;
 
 template <class R, int FVS, int RC, bool CHR>
 __device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView& W,
@@ -388,7 +394,12 @@ __device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView&
                                             int wq, int lane, long long row);
 
 template <class R, int FVS, int RC, bool CHR = false>
+#ifdef NS3D_XW_MAXREG
 __global__ void __launch_bounds__(32 * XW_WARPS)
+__maxnreg__((CHR || sizeof(R) == 8) ? 255 : NS3D_XW_MAXREG)
+#else
+__global__ void __launch_bounds__(32 * XW_WARPS)
+#endif
 k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
     __shared__ SplitRing<R, XW_WARPS, 96> ring;  // [warp][3 chunks x 32 cells]
@@ -1249,7 +1260,11 @@ __device__ __forceinline__ void fused_cell(const DevParams& P, const StateView& 
 }
 
 template <int DIR, class R, int FVS, int RC, bool FUSE>
+#ifdef NS3D_RING_MAXREG
+__global__ void __launch_bounds__(RingCfg<R>::T) __maxnreg__(sizeof(R) == 4 ? NS3D_RING_MAXREG : 255)
+#else
 __global__ void __launch_bounds__(RingCfg<R>::T, RingCfg<R>::MINB)
+#endif
 k_sweep_ring(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl* __restrict__ ctrl,
              FuseArgs<R> F) {
     static_assert(DIR == 1 || DIR == 2, "y and z sweeps");
