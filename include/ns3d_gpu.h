@@ -144,6 +144,19 @@ ns3d_status ns3d_synchronize(ns3d_ctx *ctx);
 ns3d_status ns3d_upload_primitive(ns3d_ctx *ctx, const double *rho, const double *u,
                                   const double *v, const double *w, const double *p,
                                   int layout);
+/* Starts copying the primitives that a following ns3d_upload_primitive will be
+ * given (same pointers, interior layout) into a device staging buffer on a
+ * copy stream, and returns; that upload then only waits for the copy, so a
+ * host loop that prefetches step k+1's state before stepping state k overlaps
+ * the transfer with the step. The arrays must stay valid and unchanged until
+ * that upload returns, and should be pinned (pageable memory copies
+ * synchronously). An upload with other pointers or layout ignores the prefetch.
+ * The first call allocates the staging buffer (6 n doubles). No reference
+ * counterpart (the reference's Field3D lives in host memory). Ghosted layout:
+ * accepted, no effect (the upload gathers on the host). */
+ns3d_status ns3d_prefetch_primitive(ns3d_ctx *ctx, const double *rho, const double *u,
+                                    const double *v, const double *w, const double *p,
+                                    int layout);
 /* Conserved state: conservedToPrimitive + apply_boundary + primitiveToConserved
  * (range_kutta.cpp:117-119). Also records U0. */
 ns3d_status ns3d_upload_conserved(ns3d_ctx *ctx, const double *rho, const double *rhou,

@@ -38,6 +38,7 @@ _SIGS = {
     "ns3d_device_bytes": (_i, [_vp, ctypes.POINTER(ctypes.c_size_t)]),
     "ns3d_synchronize": (_i, [_vp]),
     "ns3d_upload_primitive": (_i, [_vp, _D, _D, _D, _D, _D, _i]),
+    "ns3d_prefetch_primitive": (_i, [_vp, _D, _D, _D, _D, _D, _i]),
     "ns3d_upload_conserved": (_i, [_vp, _D, _D, _D, _D, _D, _i]),
     "ns3d_download_primitive": (_i, [_vp, _D, _D, _D, _D, _D, _D, _D, _i]),
     "ns3d_download_conserved": (_i, [_vp, _D, _D, _D, _D, _D, _i]),

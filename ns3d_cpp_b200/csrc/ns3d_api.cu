@@ -60,6 +60,16 @@ struct ns3d_ctx {
     bool fuse = false;
     long long n = 0;
     double* wmem = nullptr;      // 3 state buffers x 6 arrays x n
+    double* slot[3] = {nullptr, nullptr, nullptr};  // state buffer b: 6 arrays of n from slot[b]
+    // ns3d_prefetch_primitive: a fourth 6 n block that host copies land in on
+    // the copy stream; the upload that uses it swaps it with the current
+    // buffer's block (no device copy)
+    double* stage_mem = nullptr;
+    double* stage = nullptr;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_staged = nullptr, ev_consumed = nullptr;
+    const double* pre_h[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool prefetched = false;
     int cur = 0, rec = 0;        // current state buffer, recorded (U0) buffer
     void* tacc = nullptr;        // 5 n (R)
     void* fv = nullptr;          // viscous fluxes: 9 n doubles (FP64) or 3 n float4 (FP32)
@@ -107,7 +117,7 @@ ns3d_status fail(ns3d_ctx* c, ns3d_status s, const std::string& msg) {
             return fail(ctx, NS3D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-double* warr(ns3d_ctx* c, int buf, int a) { return c->wmem + ((long long)buf * 6 + a) * c->n; }
+double* warr(ns3d_ctx* c, int buf, int a) { return c->slot[buf] + (long long)a * c->n; }
 
 cudaEvent_t pool_event(ns3d_ctx* c) {
     if (c->ev_used == c->ev_pool.size()) {
@@ -840,6 +850,7 @@ ns3d_status ns3d_create(const ns3d_params* p, int device, ns3d_ctx** out) {
         cudaMalloc(&ctx->step_times, sizeof(double) * kStepTimesCap0) != cudaSuccess)
         return bail(NS3D_ERR_NOMEM, "device allocation failed");
     ctx->step_times_cap = kStepTimesCap0;
+    for (int b = 0; b < 3; ++b) ctx->slot[b] = ctx->wmem + (size_t)b * 6 * n;
     // a uniform quiescent state until the first upload (Field3D::allocate, :232-236)
     cudaMemsetAsync(ctx->wmem, 0, sizeof(double) * 18 * n, ctx->stream);
     if (reset_ctrl(ctx) != NS3D_OK) return bail(NS3D_ERR_CUDA, ctx->err);
@@ -853,11 +864,13 @@ ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
     if (!ctx) return NS3D_ERR_INVALID;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     if (ctx->fft_ready) cufftDestroy(ctx->fft);
     cudaFree(ctx->spec);
     cudaFree(ctx->bins);
     cudaFree(ctx->spec_part);
     cudaFree(ctx->wmem);
+    cudaFree(ctx->stage_mem);
     cudaFree(ctx->tacc);
     cudaFree(ctx->fv);
     cudaFree(ctx->ctrl);
@@ -869,6 +882,9 @@ ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->ev_staged) cudaEventDestroy(ctx->ev_staged);
+    if (ctx->ev_consumed) cudaEventDestroy(ctx->ev_consumed);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NS3D_OK;
@@ -882,13 +898,49 @@ ns3d_status ns3d_get_params(const ns3d_ctx* ctx, ns3d_params* out) {
 
 ns3d_status ns3d_device_bytes(const ns3d_ctx* ctx, size_t* bytes) {
     if (!ctx || !bytes) return NS3D_ERR_INVALID;
-    *bytes = sizeof(double) * 18 * (size_t)ctx->n + ctx->rsize * 14 * (size_t)ctx->n;
+    *bytes = sizeof(double) * (ctx->stage_mem ? 24 : 18) * (size_t)ctx->n +
+             ctx->rsize * 14 * (size_t)ctx->n;
     return NS3D_OK;
 }
 
 ns3d_status ns3d_synchronize(ns3d_ctx* ctx) {
     if (!ctx) return NS3D_ERR_INVALID;
     NS3D_CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->copy_stream) NS3D_CK(cudaStreamSynchronize(ctx->copy_stream));
+    return NS3D_OK;
+}
+
+ns3d_status ns3d_prefetch_primitive(ns3d_ctx* ctx, const double* rho, const double* u,
+                                    const double* v, const double* w, const double* p,
+                                    int layout) {
+    if (!ctx) return NS3D_ERR_INVALID;
+    const double* h[5] = {rho, u, v, w, p};
+    for (int q = 0; q < 5; ++q)
+        if (!h[q]) return fail(ctx, NS3D_ERR_INVALID, "null host pointer");
+    if (layout == NS3D_LAYOUT_GHOSTED) return NS3D_OK;  // gathered on the host at upload time
+    if (layout != NS3D_LAYOUT_INTERIOR) return fail(ctx, NS3D_ERR_INVALID, "unknown layout");
+    NS3D_CK(cudaSetDevice(ctx->device));
+    const size_t n = (size_t)ctx->n;
+    if (!ctx->stage_mem) {
+        if (cudaMalloc(&ctx->stage_mem, sizeof(double) * 6 * n) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->stage_mem = nullptr;
+            return fail(ctx, NS3D_ERR_NOMEM, "prefetch staging allocation failed");
+        }
+        ctx->stage = ctx->stage_mem;
+        NS3D_CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        NS3D_CK(cudaEventCreateWithFlags(&ctx->ev_staged, cudaEventDisableTiming));
+        NS3D_CK(cudaEventCreateWithFlags(&ctx->ev_consumed, cudaEventDisableTiming));
+    }
+    // the staging block was the current buffer's until the last upload that
+    // used a prefetch: wait until the work queued before that upload is done
+    NS3D_CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_consumed, 0));
+    for (int q = 0; q < 5; ++q)
+        NS3D_CK(cudaMemcpyAsync(ctx->stage + q * n, h[q], sizeof(double) * n,
+                                cudaMemcpyHostToDevice, ctx->copy_stream));
+    NS3D_CK(cudaEventRecord(ctx->ev_staged, ctx->copy_stream));
+    for (int q = 0; q < 5; ++q) ctx->pre_h[q] = h[q];
+    ctx->prefetched = true;
     return NS3D_OK;
 }
 
@@ -897,12 +949,22 @@ ns3d_status ns3d_upload_primitive(ns3d_ctx* ctx, const double* rho, const double
     if (!ctx) return NS3D_ERR_INVALID;
     NS3D_CK(cudaSetDevice(ctx->device));
     const double* h[5] = {rho, u, v, w, p};
-    double* d[5];
-    for (int q = 0; q < 5; ++q) d[q] = warr(ctx, ctx->cur, q);
-    ns3d_status s = upload5(ctx, h, d, layout);
-    if (s != NS3D_OK) return s;
+    bool staged = ctx->prefetched && layout == NS3D_LAYOUT_INTERIOR;
+    for (int q = 0; q < 5; ++q) staged = staged && h[q] == ctx->pre_h[q];
+    ctx->prefetched = false;
+    if (staged) {
+        // the prefetched arrays become the current buffer's
+        NS3D_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_staged, 0));
+        std::swap(ctx->slot[ctx->cur], ctx->stage);
+    } else {
+        double* d[5];
+        for (int q = 0; q < 5; ++q) d[q] = warr(ctx, ctx->cur, q);
+        ns3d_status s = upload5(ctx, h, d, layout);
+        if (s != NS3D_OK) return s;
+    }
     k_prim_finish<<<blocks_for(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->L.P, outv(ctx, ctx->cur));
     NS3D_CK(cudaGetLastError());
+    if (staged) NS3D_CK(cudaEventRecord(ctx->ev_consumed, ctx->stream));
     ctx->rec = ctx->cur;
     ctx->dtmin_valid = false;
     NS3D_CK(cudaStreamSynchronize(ctx->stream));

@@ -177,10 +177,22 @@ class Solver:
         return out
 
     def upload_primitive(self, W, layout: str = "interior") -> None:
-        """Initial condition path (main.cpp:67-71); also records U0."""
+        """Initial condition path (main.cpp:67-71); also records U0. Uses the
+        copy a prefetch_primitive of the same arrays started."""
         arrs = self._prep(W, layout)
         self._ck(self.lib.ns3d_upload_primitive(self.ctx, *[_dptr(a) for a in arrs],
                                                 LAYOUT[layout]))
+        self._prefetched = None
+
+    def prefetch_primitive(self, W, layout: str = "interior") -> None:
+        """Start copying W (float64, C-contiguous; pinned memory for overlap)
+        to the device; the next upload_primitive(W) only waits for the copy.
+        W must stay unchanged until that upload returns; the solver keeps a
+        reference to it until then."""
+        arrs = self._prep(W, layout)
+        self._ck(self.lib.ns3d_prefetch_primitive(self.ctx, *[_dptr(a) for a in arrs],
+                                                  LAYOUT[layout]))
+        self._prefetched = arrs
 
     def upload_conserved(self, U, layout: str = "interior") -> None:
         """conservedToPrimitive + apply_boundary + primitiveToConserved; records U0."""

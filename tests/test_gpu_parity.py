@@ -125,6 +125,41 @@ def test_nonphysical_state_returns_status():
         s.runge_kutta_3(1e-4)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32acc64"])
+def test_prefetched_upload_is_the_plain_upload(precision):
+    """ns3d_prefetch_primitive + ns3d_upload_primitive of the same arrays give
+    the state, and the steps from it, that a plain upload gives; a prefetch
+    issued while steps run does not disturb them; an upload of other arrays
+    ignores a pending prefetch. Each prefetched upload swaps the staging block
+    with the current buffer's, so the loop also walks the swapped buffers
+    through the RK3 buffer rotation."""
+    n = 32
+    p = params_from_cfg(ref_cfg(n), precision=precision)
+    Ws = [np.ascontiguousarray(tgv_input(n, seed=s)) for s in (1, 2, 3)]
+    with ns.Solver(p) as a, ns.Solver(p) as b:
+        base = b.device_bytes()
+        b.prefetch_primitive(Ws[0])
+        for k in range(4):
+            W, Wn = Ws[k % 3], Ws[(k + 1) % 3]
+            a.upload_primitive(W)
+            plain = a.download_primitive(with_T_c=True)
+            a.step(k + 1)
+            ref = a.download_primitive(with_T_c=True)
+            b.upload_primitive(W)  # prefetched in the previous iteration
+            assert np.array_equal(b.download_primitive(with_T_c=True), plain), k
+            b.prefetch_primitive(Wn)  # copied while the steps run
+            b.step(k + 1)
+            assert np.array_equal(b.download_primitive(with_T_c=True), ref), k
+            assert a.last_dt() == b.last_dt()
+            if k == 2:
+                other = Ws[(k + 2) % 3]
+                b.upload_primitive(other)  # not the prefetched arrays
+                a.upload_primitive(other)
+                assert np.array_equal(b.download_primitive(), a.download_primitive())
+                b.prefetch_primitive(Wn)
+        assert b.device_bytes() == base + 6 * 8 * n ** 3
+
+
 def test_conserved_upload_and_ghosted_layout(oracle_mod):
     n = 8
     cfg = ref_cfg(n)
