@@ -355,7 +355,7 @@ def adjoint_cost(torch, ns, device, nsteps=200, K=20, n=64, fd_dirs=2):
     with ns.Solver(p, device=device) as s:
         stream = torch.cuda.ExternalStream(s.stream_handle())
         s.upload_primitive(W)
-        s.adjoint(4, 2)                      # warm-up (module load, allocator)
+        s.adjoint(nsteps, K)                 # warm-up: modules, the context's checkpoint arrays
         s.upload_primitive(W)
         s.step(3)
 

@@ -214,7 +214,10 @@ ns3d_status ns3d_step_times(ns3d_ctx *ctx, double *times, int cap, int *n);
  * sw_entropy_eps > 0 to make |lambda| smooth) or Lax-Friedrichs, WENO5 or the
  * linear reconstructions, component-wise; MDCD_HYBRID and char_recon return
  * NS3D_ERR_UNSUPPORTED. Arrays are host pointers to 5 consecutive interior
- * blocks (rho, u, v, w, p). */
+ * blocks (rho, u, v, w, p). The checkpoints and scratch arrays stay in the
+ * context after a call (ns3d_device_bytes counts them): a later call that
+ * needs no more checkpoints, no larger checkpoint_every and no more steps
+ * allocates nothing. */
 
 /* lam_w = (d rhs / d w)^T lam_rhs at the current state (vector-Jacobian
  * product of compute_rhs with respect to the primitives). */

@@ -81,6 +81,10 @@ struct ns3d_ctx {
     int sums_blocks = 0;
     bool dtmin_valid = false;
     double* step_times = nullptr;  // current_time after each step of the last run call
+    // device scratch of the adjoint entry points, kept between calls (grown,
+    // never shrunk; freed with the context)
+    double* adj_buf[10] = {};
+    size_t adj_cap[10] = {};
     int step_times_cap = 0, step_times_n = 0;
     double time = 0.0, out_next = 0.0;
     long long steps = 0;         // completed steps (the time_advance step count beside `time`)
@@ -877,6 +881,7 @@ ns3d_status ns3d_destroy(ns3d_ctx* ctx) {
     cudaFree(ctx->sums_part);
     cudaFree(ctx->sums_out);
     cudaFree(ctx->step_times);
+    for (double* b : ctx->adj_buf) cudaFree(b);
     if (ctx->ctrl_host) cudaFreeHost(ctx->ctrl_host);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
@@ -900,6 +905,7 @@ ns3d_status ns3d_device_bytes(const ns3d_ctx* ctx, size_t* bytes) {
     if (!ctx || !bytes) return NS3D_ERR_INVALID;
     *bytes = sizeof(double) * (ctx->stage_mem ? 24 : 18) * (size_t)ctx->n +
              ctx->rsize * 14 * (size_t)ctx->n;
+    for (size_t c : ctx->adj_cap) *bytes += sizeof(double) * c;
     return NS3D_OK;
 }
 
@@ -1459,6 +1465,28 @@ struct DevBuf {
     bool alloc(size_t count) { return cudaMalloc(&p, sizeof(double) * count) == cudaSuccess; }
 };
 
+// The adjoint's scratch arrays, by role.
+enum { AB_CK, AB_WS, AB_LA, AB_LB, AB_LU0, AB_LR, AB_G, AB_LG, AB_DTD, AB_LW, AB_COUNT };
+
+// `count` doubles of adjoint scratch `slot`, kept in the context: a call that
+// needs no more than an earlier one allocates nothing (allocating and freeing
+// ~1 GB per call cost 0.1-0.7 s of the call, varying from call to call).
+double* adj_scratch(ns3d_ctx* c, int slot, size_t count) {
+    if (count > c->adj_cap[slot]) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->adj_buf[slot]);
+        c->adj_buf[slot] = nullptr;
+        c->adj_cap[slot] = 0;
+        if (cudaMalloc(&c->adj_buf[slot], sizeof(double) * count) != cudaSuccess) {
+            cudaGetLastError();
+            c->adj_buf[slot] = nullptr;
+            return nullptr;
+        }
+        c->adj_cap[slot] = count;
+    }
+    return c->adj_buf[slot];
+}
+
 ns3d_status adjoint_supported(ns3d_ctx* ctx) {
     if (ctx->p.precision != NS3D_PREC_FP64)
         return fail(ctx, NS3D_ERR_UNSUPPORTED, "the adjoint differentiates the FP64 form");
@@ -1483,14 +1511,15 @@ ns3d_status ns3d_rhs_vjp(ns3d_ctx* ctx, const double* lam_rhs, double* lam_w) {
     ns3d_status s = adjoint_supported(ctx);
     if (s != NS3D_OK) return s;
     const long long n = ctx->n;
-    DevBuf lr, lw, G, lg;
-    if (!lr.alloc(5 * n) || !lw.alloc(5 * n) || !G.alloc((size_t)adj_scratch_blocks(ctx->L) * n) ||
-        !lg.alloc(16 * n))
-        return fail(ctx, NS3D_ERR_NOMEM, "adjoint scratch allocation failed");
-    NS3D_CK(cudaMemcpyAsync(lr.p, lam_rhs, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, ctx->stream));
-    NS3D_CK(cudaMemsetAsync(lw.p, 0, sizeof(double) * 5 * n, ctx->stream));
-    NS3D_LAUNCH(NS3D_KERNEL_OTHER, 11, adj_rhs_vjp(ctx->L, view(ctx, ctx->cur), lr.p, G.p, lg.p, lw.p));
-    NS3D_CK(cudaMemcpyAsync(lam_w, lw.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    double* lr = adj_scratch(ctx, AB_LR, 5 * n);
+    double* lw = adj_scratch(ctx, AB_LW, 5 * n);
+    double* G = adj_scratch(ctx, AB_G, (size_t)adj_scratch_blocks(ctx->L) * n);
+    double* lg = adj_scratch(ctx, AB_LG, 16 * n);
+    if (!lr || !lw || !G || !lg) return fail(ctx, NS3D_ERR_NOMEM, "adjoint scratch allocation failed");
+    NS3D_CK(cudaMemcpyAsync(lr, lam_rhs, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, ctx->stream));
+    NS3D_CK(cudaMemsetAsync(lw, 0, sizeof(double) * 5 * n, ctx->stream));
+    NS3D_LAUNCH(NS3D_KERNEL_OTHER, 11, adj_rhs_vjp(ctx->L, view(ctx, ctx->cur), lr, G, lg, lw));
+    NS3D_CK(cudaMemcpyAsync(lam_w, lw, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->stream));
     NS3D_CK(cudaStreamSynchronize(ctx->stream));
     return NS3D_OK;
 }
@@ -1520,11 +1549,16 @@ ns3d_status ns3d_adjoint(ns3d_ctx* ctx, int nsteps, int K, const double* dts_in,
     const long long n = ctx->n;
     const size_t st = 6 * (size_t)n;  // one state: rho,u,v,w,p,T
     const int nseg = (nsteps + K - 1) / K;
-    DevBuf ck, ws, la, lb, lu0, lr, G, lg, dtd;
-    if (!ck.alloc(st * nseg) || !ws.alloc(st * (3 * (size_t)K + 1)) || !la.alloc(5 * n) ||
-        !lb.alloc(5 * n) || !lu0.alloc(5 * n) || !lr.alloc(5 * n) ||
-        !G.alloc((size_t)adj_scratch_blocks(ctx->L) * n) || !lg.alloc(16 * n) ||
-        !dtd.alloc(nsteps))
+    double* ck = adj_scratch(ctx, AB_CK, st * nseg);
+    double* ws = adj_scratch(ctx, AB_WS, st * (3 * (size_t)K + 1));
+    double* la = adj_scratch(ctx, AB_LA, 5 * n);
+    double* lb = adj_scratch(ctx, AB_LB, 5 * n);
+    double* lu0 = adj_scratch(ctx, AB_LU0, 5 * n);
+    double* lr = adj_scratch(ctx, AB_LR, 5 * n);
+    double* G = adj_scratch(ctx, AB_G, (size_t)adj_scratch_blocks(ctx->L) * n);
+    double* lg = adj_scratch(ctx, AB_LG, 16 * n);
+    double* dtd = adj_scratch(ctx, AB_DTD, nsteps);
+    if (!ck || !ws || !la || !lb || !lu0 || !lr || !G || !lg || !dtd)
         return fail(ctx, NS3D_ERR_NOMEM, "adjoint checkpoint/scratch allocation failed");
     std::vector<double> dts(nsteps);
 
@@ -1532,7 +1566,7 @@ ns3d_status ns3d_adjoint(ns3d_ctx* ctx, int nsteps, int K, const double* dts_in,
     if ((s = reset_ctrl(ctx)) != NS3D_OK) return s;
     for (int k = 0; k < nsteps; ++k) {
         if (k % K == 0)
-            NS3D_CK(cudaMemcpyAsync(ck.p + (size_t)(k / K) * st, warr(ctx, ctx->cur, 0),
+            NS3D_CK(cudaMemcpyAsync(ck + (size_t)(k / K) * st, warr(ctx, ctx->cur, 0),
                                     sizeof(double) * st, cudaMemcpyDeviceToDevice, ctx->stream));
         ctx->rec = ctx->cur;
         if (dts_in) {
@@ -1546,11 +1580,11 @@ ns3d_status ns3d_adjoint(ns3d_ctx* ctx, int nsteps, int K, const double* dts_in,
                         (k_control_pre<<<1, 1, 0, ctx->stream>>>(ctx->ctrl, 0, ctx->p.cfl,
                                                                   ctx->p.dt_fixed, 0.0, 0.0)));
         }
-        NS3D_CK(cudaMemcpyAsync(dtd.p + k, &ctx->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice,
+        NS3D_CK(cudaMemcpyAsync(dtd + k, &ctx->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice,
                                 ctx->stream));
         if ((s = enqueue_rk3(ctx)) != NS3D_OK) return s;
     }
-    NS3D_CK(cudaMemcpyAsync(dts.data(), dtd.p, sizeof(double) * nsteps, cudaMemcpyDeviceToHost,
+    NS3D_CK(cudaMemcpyAsync(dts.data(), dtd, sizeof(double) * nsteps, cudaMemcpyDeviceToHost,
                             ctx->stream));
     if ((s = read_ctrl(ctx)) != NS3D_OK) return s;
     if (ctx->ctrl_host->bad_cell < n) return fail(ctx, NS3D_ERR_NONPHYSICAL, "non-physical state");
@@ -1561,8 +1595,8 @@ ns3d_status ns3d_adjoint(ns3d_ctx* ctx, int nsteps, int K, const double* dts_in,
     if (J) *J = sums[0] * (ctx->p.dx * ctx->p.dy * ctx->p.dz);
 
     // ---- seed: dJ/dw at the end state ----
-    double* A = la.p;
-    double* B = lb.p;
+    double* A = la;
+    double* B = lb;
     if (lam_final)
         NS3D_CK(cudaMemcpyAsync(A, lam_final, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, ctx->stream));
     else
@@ -1572,26 +1606,26 @@ ns3d_status ns3d_adjoint(ns3d_ctx* ctx, int nsteps, int K, const double* dts_in,
     // ---- reverse sweep, segment by segment ----
     for (int seg = nseg - 1; seg >= 0; --seg) {
         const int s0 = seg * K, m = std::min(K, nsteps - s0);
-        NS3D_CK(cudaMemcpyAsync(ws.p, ck.p + (size_t)seg * st, sizeof(double) * st,
+        NS3D_CK(cudaMemcpyAsync(ws, ck + (size_t)seg * st, sizeof(double) * st,
                                 cudaMemcpyDeviceToDevice, ctx->stream));
         for (int j = 0; j < m; ++j) {  // recompute the segment's stage states
-            double* w0 = ws.p + (size_t)(3 * j) * st;
+            double* w0 = ws + (size_t)(3 * j) * st;
             if ((s = set_dt(ctx, dts[s0 + j])) != NS3D_OK) return s;
             if ((s = stage_at(ctx, 1, w0, w0, w0 + st)) != NS3D_OK) return s;
             if ((s = stage_at(ctx, 2, w0 + st, w0, w0 + 2 * st)) != NS3D_OK) return s;
             if ((s = stage_at(ctx, 3, w0 + 2 * st, w0, w0 + 3 * st)) != NS3D_OK) return s;
         }
         for (int j = m - 1; j >= 0; --j) {  // A: adjoint of the step's end state
-            double* w0 = ws.p + (size_t)(3 * j) * st;
+            double* w0 = ws + (size_t)(3 * j) * st;
             const double dt = dts[s0 + j];
             for (int stg = 3; stg >= 1; --stg) {
                 const StateView Wk = view_at(w0 + (size_t)stg * st, n);
                 const StateView Wp = view_at(w0 + (size_t)(stg - 1) * st, n);
-                NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1, adj_stage(ctx->L, stg, Wk, Wp, A, lu0.p, lr.p, B, dt));
-                NS3D_LAUNCH(NS3D_KERNEL_OTHER, 11, adj_rhs_vjp(ctx->L, Wp, lr.p, G.p, lg.p, B));
+                NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1, adj_stage(ctx->L, stg, Wk, Wp, A, lu0, lr, B, dt));
+                NS3D_LAUNCH(NS3D_KERNEL_OTHER, 11, adj_rhs_vjp(ctx->L, Wp, lr, G, lg, B));
                 std::swap(A, B);
             }
-            NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1, adj_finish(ctx->L, view_at(w0, n), lu0.p, A));
+            NS3D_LAUNCH(NS3D_KERNEL_OTHER, 1, adj_finish(ctx->L, view_at(w0, n), lu0, A));
         }
     }
     NS3D_CK(cudaMemcpyAsync(grad, A, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, ctx->stream));
