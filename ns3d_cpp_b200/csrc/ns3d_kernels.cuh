@@ -790,6 +790,17 @@ k_visc_flux_25d(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __rest
 // Each thread owns its staging slots (halo cells h = tid, tid + NT, ...), so
 // the staged values need no barrier, only the thread's own wait.
 // ---------------------------------------------------------------------------
+// Two values of type R in one 8- / 16-byte word.
+template <class R> struct Pair;
+template <> struct Pair<float> {
+    using type = float2;
+    __device__ static float2 make(float a, float b) { return make_float2(a, b); }
+};
+template <> struct Pair<double> {
+    using type = double2;
+    __device__ static double2 make(double a, double b) { return make_double2(a, b); }
+};
+
 template <class R>
 struct VPipe {
     using T = VTile<R>;
@@ -832,7 +843,25 @@ k_visc_flux_pipe(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __res
     if (ctrl && ctrl->stop) return;
     constexpr bool kDeviation = sizeof(R) < sizeof(double);
     extern __shared__ __align__(16) unsigned char vsm[];
+    // FP32: the tile holds (u, v) and (w, T) as float2 pairs, so one 8-byte
+    // shared load feeds two derivatives (0.400 -> 0.380 ms at 256^3); FP64
+    // keeps one array per variable (16-byte pairs measured slower, 0.79 -> 0.83)
+    constexpr bool kPairs = sizeof(R) == 4;
+    using R2 = typename Pair<R>::type;
+    R2 (*tile2)[2][SY][SX] = reinterpret_cast<R2 (*)[2][SY][SX]>(vsm);       // [2][2][SY][SX]
     R (*tile)[4][SY][SX] = reinterpret_cast<R (*)[4][SY][SX]>(vsm);          // [2][4][SY][SX]
+    // tile cell (flat index t of buffer buf) <- the four values of one cell
+    auto put = [&](int buf, int t, R a, R b, R c, R d) {
+        if constexpr (kPairs) {
+            (&tile2[buf][0][0][0])[t] = Pair<R>::make(a, b);
+            (&tile2[buf][1][0][0])[t] = Pair<R>::make(c, d);
+        } else {
+            (&tile[buf][0][0][0])[t] = a;
+            (&tile[buf][1][0][0])[t] = b;
+            (&tile[buf][2][0][0])[t] = c;
+            (&tile[buf][3][0][0])[t] = d;
+        }
+    };
     double (*sth)[NH] = reinterpret_cast<double (*)[NH]>(vsm + VP::tile_bytes);  // [4][NH]
     double (*stq)[NT] = reinterpret_cast<double (*)[NT]>(vsm + VP::tile_bytes + sizeof(double) * 4 * NH);
     const int nx = P.nx, ny = P.ny, nz = P.nz;
@@ -858,7 +887,6 @@ k_visc_flux_pipe(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __res
         hti[c] = ly * SX + lx;
         hoff[c] = wrap1(j0 - H + ly, ny) * nx + wrap1(i0 - H + lx, nx);
     }
-    auto tflat = [&](int buf, int v) { return &tile[buf][v][0][0]; };
     const long long col = (long long)j * nx + i;
     auto issue = [&](int kh, int kq) {  // halo of plane kh, queue head of plane kq
 #pragma unroll
@@ -888,12 +916,12 @@ k_visc_flux_pipe(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __res
         const int h = tid + c * NT;
         if (h < NH) {
             const long long off = (long long)k0 * sxy + hoff[c];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) tflat(0, v)[hti[c]] = R(src[v][off] - ref[v]);
+            put(0, hti[c], R(src[0][off] - ref[0]), R(src[1][off] - ref[1]), R(src[2][off] - ref[2]),
+                R(src[3][off] - ref[3]));
         }
     }
-#pragma unroll
-    for (int v = 0; v < 4; ++v) tile[0][v][ty + H][tx + H] = q[v][4];
+    const int tc = (ty + H) * SX + tx + H;  // this thread's cell in the tile
+    put(0, tc, q[0][4], q[1][4], q[2][4], q[3][4]);
     issue(k0 + 1, k0 + 4);
     __syncthreads();
     const R dx = R(P.dx), dy = R(P.dy), dz = R(P.dz);
@@ -909,23 +937,38 @@ k_visc_flux_pipe(DevParams P, StateView W, R* __restrict__ fv, const Ctrl* __res
 #pragma unroll
             for (int c = 0; c < HPT; ++c) {
                 const int h = tid + c * NT;
-                if (h < NH) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) tflat(b ^ 1, v)[hti[c]] = R(sth[v][h] - ref[v]);
-                }
+                if (h < NH)
+                    put(b ^ 1, hti[c], R(sth[0][h] - ref[0]), R(sth[1][h] - ref[1]),
+                        R(sth[2][h] - ref[2]), R(sth[3][h] - ref[3]));
             }
-#pragma unroll
-            for (int v = 0; v < 4; ++v) tile[b ^ 1][v][ty + H][tx + H] = q[v][5];
+            put(b ^ 1, tc, q[0][5], q[1][5], q[2][5], q[3][5]);
             issue(k + 2, k + 5);
         }
         const int cx = tx + H, cy = ty + H;
         R g[4][3];
+        if constexpr (kPairs) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            g[v][0] = dcentral<R, ORD>([&](int o) { return tile[b][v][cy][cx + o]; }, dx);
-            g[v][1] = dcentral<R, ORD>([&](int o) { return tile[b][v][cy + o][cx]; }, dy);
-            g[v][2] = dcentral<R, ORD>([&](int o) { return q[v][4 + o]; }, dz);
+            for (int pr = 0; pr < 2; ++pr) {
+#pragma unroll
+                for (int d = 0; d < 2; ++d) {  // x, then y taps of one pair
+                    R2 t2[2 * H + 1];
+#pragma unroll
+                    for (int o = -H; o <= H; ++o)
+                        if (o != 0) t2[o + H] = d == 0 ? tile2[b][pr][cy][cx + o] : tile2[b][pr][cy + o][cx];
+                    const R h = d == 0 ? dx : dy;
+                    g[2 * pr][d] = dcentral<R, ORD>([&](int o) { return t2[o + H].x; }, h);
+                    g[2 * pr + 1][d] = dcentral<R, ORD>([&](int o) { return t2[o + H].y; }, h);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                g[v][0] = dcentral<R, ORD>([&](int o) { return tile[b][v][cy][cx + o]; }, dx);
+                g[v][1] = dcentral<R, ORD>([&](int o) { return tile[b][v][cy + o][cx]; }, dy);
+            }
         }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) g[v][2] = dcentral<R, ORD>([&](int o) { return q[v][4 + o]; }, dz);
         const R du_dx = g[0][0], du_dy = g[0][1], du_dz = g[0][2];
         const R dv_dx = g[1][0], dv_dy = g[1][1], dv_dz = g[1][2];
         const R dw_dx = g[2][0], dw_dy = g[2][1], dw_dz = g[2][2];
@@ -1195,8 +1238,14 @@ __device__ __forceinline__ void stage_cell(const DevParams& P, const StateView& 
 // are latency-bound, and more resident warps beat more loads in flight per
 // thread. Measured at 256^3: FP32 0.713 -> 0.578 ms (5 blocks 0.630, 7 blocks
 // 0.609, 10 blocks 0.680); FP64 1.80 -> 1.39 ms (6 blocks 1.52, 10 blocks 1.55).
+#ifndef NS3D_UPD3_MINB_F32
+#define NS3D_UPD3_MINB_F32 8
+#endif
+#ifndef NS3D_UPD3_MINB_F64
+#define NS3D_UPD3_MINB_F64 8
+#endif
 template <class R, int ORD, int STAGE>
-__global__ void __launch_bounds__(128, 8)
+__global__ void __launch_bounds__(128, STAGE != 3 ? 8 : (sizeof(R) == 4 ? NS3D_UPD3_MINB_F32 : NS3D_UPD3_MINB_F64))
 k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
          const R* __restrict__ fv, StateOut Wn, Ctrl* ctrl) {
     if (ctrl->stop) return;
