@@ -1238,14 +1238,8 @@ __device__ __forceinline__ void stage_cell(const DevParams& P, const StateView& 
 // are latency-bound, and more resident warps beat more loads in flight per
 // thread. Measured at 256^3: FP32 0.713 -> 0.578 ms (5 blocks 0.630, 7 blocks
 // 0.609, 10 blocks 0.680); FP64 1.80 -> 1.39 ms (6 blocks 1.52, 10 blocks 1.55).
-#ifndef NS3D_UPD3_MINB_F32
-#define NS3D_UPD3_MINB_F32 8
-#endif
-#ifndef NS3D_UPD3_MINB_F64
-#define NS3D_UPD3_MINB_F64 8
-#endif
 template <class R, int ORD, int STAGE>
-__global__ void __launch_bounds__(128, STAGE != 3 ? 8 : (sizeof(R) == 4 ? NS3D_UPD3_MINB_F32 : NS3D_UPD3_MINB_F64))
+__global__ void __launch_bounds__(128, 8)
 k_update(DevParams P, StateView Wc, StateView W0, const R* __restrict__ tacc,
          const R* __restrict__ fv, StateOut Wn, Ctrl* ctrl) {
     if (ctrl->stop) return;
