@@ -298,7 +298,7 @@ def error_run(ns, n, W, steps, device):
             "reference": "FP64 form of this code (itself 1e-12 parity with the oracle)"}
 
 
-def e2e_run(torch, ns, n, W, steps, device, prefetch=True):
+def e2e_run(torch, ns, n, W, steps, device, prefetch=True, dist=None, use_cuda=True, world=1):
     """Same metric through the public API with host buffers: every step uploads
     its inputs (the state) from pinned host memory, steps, and reads the total
     energy back. With `prefetch`, step k+1's upload is started (on the
@@ -317,6 +317,7 @@ def e2e_run(torch, ns, n, W, steps, device, prefetch=True):
             s.compute_total_energy()
         s.synchronize()
         torch.cuda.synchronize()
+        dist_barrier(dist, use_cuda)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
@@ -331,13 +332,17 @@ def e2e_run(torch, ns, n, W, steps, device, prefetch=True):
         e1.synchronize()
         wall = time.perf_counter() - t0
         ms = e0.elapsed_time(e1)
+    dist_barrier(dist, use_cuda)
+    ms = dist_max(dist, ms, use_cuda)
+    wall = dist_max(dist, wall, use_cuda)
     h2d = 5 * W[0].size * 8
     d2h = 12 * 8
     path = ("Solver.upload_primitive(pinned host; the next step's prefetch_primitive overlapping "
             "this step) + step(1) + compute_total_energy" if prefetch else
             "Solver.upload_primitive(pinned host) + step(1) + compute_total_energy")
-    return {"value": steps / (ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "wall_steps_per_s": steps / wall, "path": path}
+    # whole job: every rank runs its own replica; the slowest rank's time
+    return {"value": world * steps / (ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "wall_steps_per_s": world * steps / wall, "path": path}
 
 
 def adjoint_cost(torch, ns, device, nsteps=200, K=20, n=64, fd_dirs=2):
@@ -488,18 +493,22 @@ def our_arm(args, rank, world, local):
         ms64_max = dist_max(dist, ms64, use_cuda)
         fp64_sps = world * k64 / (ms64_max / 1e3)
 
+    # --- end to end through the public API, host buffers, on every rank ---
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = e2e_run(torch, ns, n, W, args.e2e_steps, local, dist=dist, use_cuda=use_cuda,
+                      world=world)
+        # the same loop with each upload issued only after the previous step
+        # has returned (no transfer/compute overlap), for comparison
+        e2e["serial_steps_per_s"] = e2e_run(torch, ns, n, W, args.e2e_steps, local, prefetch=False,
+                                            dist=dist, use_cuda=use_cuda, world=world)["value"]
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
 
     errors = error_run(ns, n, W, args.err_steps, local) if args.err_steps > 0 else None
-    e2e = e2e_run(torch, ns, n, W, args.e2e_steps, local) if args.e2e_steps > 0 else None
-    if e2e is not None:
-        # the same loop with each upload issued only after the previous step
-        # has returned (no transfer/compute overlap), for comparison
-        e2e["serial_steps_per_s"] = e2e_run(torch, ns, n, W, args.e2e_steps, local,
-                                            prefetch=False)["value"]
     adjoint = None if args.skip_adjoint else adjoint_cost(torch, ns, local)
 
     # dominant kernel roofline (per launch, CUDA-event timed in the timed region)
