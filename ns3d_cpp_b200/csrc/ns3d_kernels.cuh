@@ -394,12 +394,7 @@ __device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView&
                                             int wq, int lane, long long row);
 
 template <class R, int FVS, int RC, bool CHR = false>
-#ifdef NS3D_XW_MAXREG
 __global__ void __launch_bounds__(32 * XW_WARPS)
-__maxnreg__((CHR || sizeof(R) == 8) ? 255 : NS3D_XW_MAXREG)
-#else
-__global__ void __launch_bounds__(32 * XW_WARPS)
-#endif
 k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
     if (ctrl && ctrl->stop) return;
     __shared__ SplitRing<R, XW_WARPS, 96> ring;  // [warp][3 chunks x 32 cells]
@@ -407,6 +402,21 @@ k_sweep_x_warp(DevParams P, StateView W, R* __restrict__ tacc, const Ctrl* __res
     const long long row = (long long)blockIdx.x * XW_WARPS + wq;
     if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
     x_sweep_row<R, FVS, RC, CHR>(P, W, tacc, ring, wq, lane, row);
+}
+
+// The FP32 component-wise form of k_sweep_x_warp, capped at 128 registers
+// (4 blocks of 128 threads per SM): left to itself the compiler takes 154 and
+// fits 3 blocks (measured at 256^3: 0.502 ms uncapped, 0.483 ms capped, with
+// 8 / 12 bytes of spills).
+template <int FVS, int RC>
+__global__ void __maxnreg__(128)
+k_sweep_x_warp_f32(DevParams P, StateView W, float* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
+    if (ctrl && ctrl->stop) return;
+    __shared__ SplitRing<float, XW_WARPS, 96> ring;
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const long long row = (long long)blockIdx.x * XW_WARPS + wq;
+    if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
+    x_sweep_row<float, FVS, RC, false>(P, W, tacc, ring, wq, lane, row);
 }
 
 // The x sweep of one periodic row by one warp (the body of k_sweep_x_warp).
@@ -535,10 +545,11 @@ __device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView&
     put(1, firstp, firstm);
     if (nch > 1) load_raw(1, nxt);
     __syncwarp();
-    // the face on the -x side of cell 0 (face nx-1 by periodicity); with one
-    // chunk per row it is lane 31's own face, taken by shuffle below
+    // the face on the -x side of cell 0 is face nx-1 (periodicity): the last
+    // chunk's lane 31 computes it from the same window, so lane 0 parks its
+    // chunk-0 face in T_acc and finishes that cell after the last chunk; with
+    // one chunk per row it is lane 31's own face, taken by shuffle below
     R carry[5] = {R(0), R(0), R(0), R(0), R(0)};
-    if (nch > 1) face_at(1, -1, 0, carry);
     int cur = 1;
     for (int c = 0; c < nch; ++c) {
         const int nslot = cur == 2 ? 0 : cur + 1;
@@ -559,6 +570,7 @@ __device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView&
         __syncwarp();
         R face[5];
         face_at(cur, lane, c, face);
+        const bool park = c == 0 && lane == 0 && nch > 1;
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             R left = __shfl_up_sync(0xffffffffu, face[q], 1);
@@ -566,9 +578,17 @@ __device__ __forceinline__ void x_sweep_row(const DevParams& P, const StateView&
             if (lane == 0) left = nch == 1 ? last : carry[q];
             carry[q] = last;
             const R d = face[q] - left;
-            tacc[q * n + id] = d * inv_h;
+            tacc[q * n + id] = park ? face[q] : d * inv_h;
         }
         cur = nslot;
+    }
+    if (nch > 1 && lane == 0) {
+        // cell 0: its parked face minus face nx-1 (the last chunk's lane 31)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const R d = tacc[q * n + base] - carry[q];
+            tacc[q * n + base] = d * inv_h;
+        }
     }
 }
 

@@ -90,7 +90,10 @@ cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl
     if (DIR == 0 && P.nx % 32 == 0) {
         const long long rows = (long long)P.ny * P.nz;
         const unsigned blocks = (unsigned)((rows + XW_WARPS - 1) / XW_WARPS);
-        k_sweep_x_warp<R, FVS, RC, CHR><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
+        if constexpr (sizeof(R) == 4 && !CHR)
+            k_sweep_x_warp_f32<FVS, RC><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
+        else
+            k_sweep_x_warp<R, FVS, RC, CHR><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
         return cudaGetLastError();
     }
     if constexpr (DIR != 0 && !CHR) {
