@@ -193,15 +193,35 @@ __device__ __forceinline__ double sqrt_nr(double b) {
     return fma(0.5 * y, fma(-s, s, b), s);
 }
 
+// sqrt_nr<1> without a branch, for code whose instructions the compiler should
+// be free to interleave with independent work (a branch ends the scheduling
+// region). Equal to sqrt_nr<1> for b in (0, 1e300); +-0 and NaN as IEEE sqrt;
+// negative b gives NaN like sqrt; b >= 1e300 or subnormal also gives NaN
+// (a sound speed or entropy-fix argument outside (1e-308, 1e300) belongs to a
+// nonphysical state, which the stage update's positivity check then reports).
+__device__ __forceinline__ double sqrt_nr_nb(double b) {
+    const bool ok = b > 0.0 && b < 1.0e300;
+    const double bs = ok ? b : 1.0;
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(bs));
+    const double s = bs * y;
+    const double r = fma(0.5 * y, fma(-s, s, bs), s);
+    return ok ? r : (b == 0.0 ? b : __longlong_as_double(0x7ff8000000000000LL));
+}
+
 // raw = (rho, u, v, w, p) of one cell; inv_gm1 = 1/(gamma-1), inv_2g = 1/(2 gamma).
 // The face normal (N1, N2, N3) is a coordinate axis, so the normal velocity is
 // one component and the c-terms enter only the normal momentum; the products
 // with the zero components (which IEEE arithmetic cannot drop by itself) are
-// left out.
-template <int FVS, int N1, int N2, int N3, int STEPS = 1>
+// left out. ENT: -1 reads whether the entropy fix is on from P.sw_eps at run
+// time, 0 / 1 fix it at compile time; NB (with STEPS = 1) takes the square
+// roots from sqrt_nr_nb, so that with ENT >= 0 the split has no branch.
+template <int FVS, int N1, int N2, int N3, int STEPS = 1, int ENT = -1, bool NB = false>
 __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, double inv_2g,
                                            const double* raw, double Fp[5], double Fm[5]) {
     static_assert(N1 + N2 + N3 == 1, "axis-aligned face normal");
+    static_assert(!NB || STEPS == 1, "the branch-free square root takes one Newton step");
+    auto root = [](double b) { return NB ? sqrt_nr_nb(b) : sqrt_nr<STEPS>(b); };
     double rho = raw[0];
     if (rho <= 0.0) rho = 1e-12;
     const double u = raw[1], v = raw[2], w = raw[3], p = raw[4];
@@ -209,14 +229,15 @@ __device__ __forceinline__ void split_fast(const DevParams& P, double inv_gm1, d
     const double ir = rcp_nr<STEPS>(rho);
     const double kinetic = 0.5 * (u * u + v * v + w * w);
     const double E = rho * (p * ir * inv_gm1 + kinetic);
-    const double c = sqrt_nr<STEPS>(gamma * p * ir);
+    const double c = root(gamma * p * ir);
     const double un = N1 ? u : (N2 ? v : w);
     if constexpr (FVS == FV_SW) {
         const double eps = P.sw_eps;
+        const bool fix = ENT < 0 ? eps > 0.0 : ENT == 1;
         const double l1 = un - c, l2 = un, l3 = un + c;
-        const double a1 = eps > 0.0 ? sqrt_nr<STEPS>(l1 * l1 + eps * eps) : fabs(l1);
-        const double a2 = eps > 0.0 ? sqrt_nr<STEPS>(l2 * l2 + eps * eps) : fabs(l2);
-        const double a3 = eps > 0.0 ? sqrt_nr<STEPS>(l3 * l3 + eps * eps) : fabs(l3);
+        const double a1 = fix ? root(l1 * l1 + eps * eps) : fabs(l1);
+        const double a2 = fix ? root(l2 * l2 + eps * eps) : fabs(l2);
+        const double a3 = fix ? root(l3 * l3 + eps * eps) : fabs(l3);
         const double l1p = 0.5 * (l1 + a1), l1m = 0.5 * (l1 - a1);
         const double l2p = 0.5 * (l2 + a2), l2m = 0.5 * (l2 - a2);
         const double l3p = 0.5 * (l3 + a3), l3m = 0.5 * (l3 - a3);
@@ -510,7 +531,24 @@ __device__ __forceinline__ R reconstruct(const R* s, const R* lin, R disp, R dis
         return lin[0] * s[0] + lin[1] * s[1] + lin[2] * s[2] + lin[3] * s[3] + lin[4] * s[4] +
                lin[5] * s[5];
     } else if constexpr (RC == RC_MDCD_HYBRID) {
-        return mdcd_hybrid(s, lin, disp, diss);
+        if constexpr (sizeof(R) == 4) {
+            // FP32-stencil form: the hybrid scheme in double on the (exactly
+            // converted) float window. Its sixth-order indicator beta3 sums
+            // products with integer weights up to 3.6e7 that cancel to a value
+            // of order (h f')^2, and tau6 = |beta3 - (beta0 + 4 beta1 +
+            // beta2) / 6| cancels further (to order h^6): in float beta3 carries
+            // ~1% and tau6 ~10% error, which moved the RHS by ~2e-3 against
+            // the FP64 form.
+            double sd[6], ld[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                sd[m] = double(s[m]);
+                ld[m] = double(lin[m]);
+            }
+            return R(mdcd_hybrid<double>(sd, ld, double(disp), double(diss)));
+        } else {
+            return mdcd_hybrid(s, lin, disp, diss);
+        }
     } else {
         return lin[0] * s[0] + lin[1] * s[1] + lin[2] * s[2] + lin[3] * s[3] + lin[4] * s[4] +
                lin[5] * s[5] + lin[6] * s[6] + lin[7] * s[7];

@@ -19,6 +19,7 @@
 #pragma once
 
 #include "ns3d_device.cuh"
+#include <type_traits>
 
 namespace ns3d {
 
@@ -417,6 +418,157 @@ k_sweep_x_warp_f32(DevParams P, StateView W, float* __restrict__ tacc, const Ctr
     const long long row = (long long)blockIdx.x * XW_WARPS + wq;
     if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
     x_sweep_row<float, FVS, RC, false>(P, W, tacc, ring, wq, lane, row);
+}
+
+// FP32-form x sweep with the split software-pipelined (rows of at least four
+// 32-cell chunks). A warp's ring has four rotating chunk slots (chunk k in
+// slot k mod 4) and a fifth that keeps chunk 0 for the last chunk's +x
+// neighbour. While the faces of chunk c are reconstructed from chunks c-1, c,
+// c+1, the split of chunk c+2 runs beside them (independent chains, no
+// branch: ENT fixes the entropy-fix choice, square roots from sqrt_nr_nb) and
+// goes into the slot of chunk c-2, which no lane reads any more; one
+// __syncwarp per chunk then makes it visible. Chunk 0's double split serves
+// as the row's offset (lane 0's value). Faces, the periodic seam and the
+// T_acc writes as in x_sweep_row.
+template <int FVS, int RC, int ENT>
+__global__ void __launch_bounds__(32 * XW_WARPS, 4)
+k_sweep_x_pipe(DevParams P, StateView W, float* __restrict__ tacc, const Ctrl* __restrict__ ctrl) {
+    if (ctrl && ctrl->stop) return;
+    constexpr int S = Stencil<RC>::S;
+    constexpr int MID = (S - 1) / 2;
+    __shared__ SplitRing<float, XW_WARPS, 160> ring;  // [warp][5 slots x 32 cells]
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const long long row = (long long)blockIdx.x * XW_WARPS + wq;
+    if (row >= (long long)P.ny * P.nz) return;  // warp-uniform
+    const int nx = P.nx;
+    const long long n = P.n;
+    const long long base = row * nx;
+    const int nch = nx >> 5;  // >= 4 (the launcher's condition)
+    float lin[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) lin[m] = float(P.lin[m]);
+    const float disp = float(P.mdcd_disp), diss = float(P.mdcd_diss);
+    const float inv_h = float(P.inv_dx);
+    const double inv_gm1 = 1.0 / (P.gamma - 1.0);
+    const double inv_2g = 1.0 / (2.0 * P.gamma);
+    double refp[5], refm[5];
+    auto load_raw = [&](int chunk, double* raw) {
+        const long long id = base + (chunk << 5) + lane;
+        raw[0] = W.rho[id];
+        raw[1] = W.u[id];
+        raw[2] = W.v[id];
+        raw[3] = W.w[id];
+        raw[4] = W.p[id];
+    };
+    auto split_d = [&](const double* raw, double* Fpd, double* Fmd) {
+        split_fast<FVS, 1, 0, 0, 1, ENT, true>(P, inv_gm1, inv_2g, raw, Fpd, Fmd);
+    };
+    auto split_raw = [&](const double* raw, float* Fp, float* Fm) {
+        double Fpd[5], Fmd[5];
+        split_d(raw, Fpd, Fmd);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            Fp[q] = float(Fpd[q] - refp[q]);
+            Fm[q] = float(Fmd[q] - refm[q]);
+        }
+    };
+    auto put = [&](int slot, const float* Fp, const float* Fm) {
+        ring.put(wq, slot * 32 + lane, Fp, Fm);
+    };
+
+    // prologue: chunk 0 (slots 0 and 4; lane 0's split is the offset), the last
+    // chunk (slot 3, as chunk -1) and chunk 1 (slot 1); chunk 2's loads issued
+    double raw[5], nxt[5];
+    {
+        float Fp[5], Fm[5];
+        double Fpd[5], Fmd[5];
+        load_raw(0, raw);
+        split_d(raw, Fpd, Fmd);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            refp[q] = __shfl_sync(0xffffffffu, Fpd[q], 0);
+            refm[q] = __shfl_sync(0xffffffffu, Fmd[q], 0);
+            Fp[q] = float(Fpd[q] - refp[q]);
+            Fm[q] = float(Fmd[q] - refm[q]);
+        }
+        put(0, Fp, Fm);
+        put(4, Fp, Fm);
+        load_raw(nch - 1, raw);
+        split_raw(raw, Fp, Fm);
+        put(3, Fp, Fm);
+        load_raw(1, raw);
+        split_raw(raw, Fp, Fm);
+        put(1, Fp, Fm);
+    }
+    load_raw(2, nxt);
+    __syncwarp();
+    float carry[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    // one chunk: faces of chunk c from chunks c-1, c, c+1; with SPLIT, chunk
+    // c+2's split beside them
+    auto chunk_step = [&](int c, auto split_tag) {
+        constexpr bool SPLIT = decltype(split_tag)::value;
+        const int sp = (c + 3) & 3, sc = c & 3, sn = c + 1 == nch ? 4 : ((c + 1) & 3);
+        double cr[5];
+        if constexpr (SPLIT) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) cr[q] = nxt[q];
+            load_raw(min(c + 3, nch - 1), nxt);
+        }
+        int cell[S];
+#pragma unroll
+        for (int m = 0; m < S; ++m) {
+            const int o = lane - MID + m;
+            const int sl = o < 0 ? sp : (o >= 32 ? sn : sc);
+            cell[m] = sl * 32 + (o & 31);
+        }
+        float face[5], Fp[5], Fm[5];
+        if constexpr (RC == RC_WENO5) {
+            float fp[S][5], fm[S][5];
+#pragma unroll
+            for (int m = 0; m < S; ++m) ring.get(wq, cell[m], fp[m], fm[m]);
+            if constexpr (SPLIT) split_raw(cr, Fp, Fm);
+            weno5_face_x2([&](int m, int q) { return fp[m][q]; },
+                          [&](int m, int q) { return fm[S - 1 - m][q]; }, face);
+        } else {
+            if constexpr (SPLIT) split_raw(cr, Fp, Fm);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                float a[S], b[S];
+#pragma unroll
+                for (int m = 0; m < S; ++m) {
+                    a[m] = ring.comp(wq, cell[m], q, false);
+                    b[m] = ring.comp(wq, cell[S - 1 - m], q, true);
+                }
+                const float plus_face = reconstruct<float, RC>(a, lin, disp, diss);
+                const float minus_face = reconstruct<float, RC>(b, lin, disp, diss);
+                face[q] = plus_face + minus_face;
+            }
+        }
+        if constexpr (SPLIT) {
+            put((c + 2) & 3, Fp, Fm);  // the slot of chunk c-2
+            __syncwarp();
+        }
+        const long long id = base + (c << 5) + lane;
+        const bool park = c == 0 && lane == 0;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            float left = __shfl_up_sync(0xffffffffu, face[q], 1);
+            const float last = __shfl_sync(0xffffffffu, face[q], 31);
+            if (lane == 0) left = carry[q];
+            carry[q] = last;
+            tacc[q * n + id] = park ? face[q] : (face[q] - left) * inv_h;
+        }
+    };
+    for (int c = 0; c + 2 < nch; ++c) chunk_step(c, std::true_type{});
+    for (int c = nch - 2; c < nch; ++c) chunk_step(c, std::false_type{});
+    if (lane == 0) {
+        // cell 0: its parked face minus face nx-1 (the last chunk's lane 31)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const float d = tacc[q * n + base] - carry[q];
+            tacc[q * n + base] = d * inv_h;
+        }
+    }
 }
 
 // The x sweep of one periodic row by one warp (the body of k_sweep_x_warp).
