@@ -531,24 +531,7 @@ __device__ __forceinline__ R reconstruct(const R* s, const R* lin, R disp, R dis
         return lin[0] * s[0] + lin[1] * s[1] + lin[2] * s[2] + lin[3] * s[3] + lin[4] * s[4] +
                lin[5] * s[5];
     } else if constexpr (RC == RC_MDCD_HYBRID) {
-        if constexpr (sizeof(R) == 4) {
-            // FP32-stencil form: the hybrid scheme in double on the (exactly
-            // converted) float window. Its sixth-order indicator beta3 sums
-            // products with integer weights up to 3.6e7 that cancel to a value
-            // of order (h f')^2, and tau6 = |beta3 - (beta0 + 4 beta1 +
-            // beta2) / 6| cancels further (to order h^6): in float beta3 carries
-            // ~1% and tau6 ~10% error, which moved the RHS by ~2e-3 against
-            // the FP64 form.
-            double sd[6], ld[6];
-#pragma unroll
-            for (int m = 0; m < 6; ++m) {
-                sd[m] = double(s[m]);
-                ld[m] = double(lin[m]);
-            }
-            return R(mdcd_hybrid<double>(sd, ld, double(disp), double(diss)));
-        } else {
-            return mdcd_hybrid(s, lin, disp, diss);
-        }
+        return mdcd_hybrid(s, lin, disp, diss);
     } else {
         return lin[0] * s[0] + lin[1] * s[1] + lin[2] * s[2] + lin[3] * s[3] + lin[4] * s[4] +
                lin[5] * s[5] + lin[6] * s[6] + lin[7] * s[7];

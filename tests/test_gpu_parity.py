@@ -290,8 +290,7 @@ def test_init_isotropic_matches_reference_golden():
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(fvs_type="LaxFriedrichs", recon="MDCD"),
-                                dict(recon="UPWIND_7TH"),
-                                dict(vis_scheme="C6th", recon="MDCD_HYBRID")], ids=scheme_id)
+                                dict(recon="UPWIND_7TH")], ids=scheme_id)
 def test_fp32_stencils_close_to_fp64(oracle_mod, kw):
     """FP32-stencil form against the FP64 oracle on Taylor-Green at Ma = 0.1,
     the hardest case for float: each split flux carries O(c/u) ~ 10x more than

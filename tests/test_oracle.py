@@ -272,3 +272,29 @@ def test_spectrum_and_stats_match_reference_golden(oracle_mod):
         assert abs(s6[name] - stats[name]) <= 1e-7 * abs(stats[name]), name
     assert abs(s["dissipation"] - stats["dissipation"]) <= 1e-5 * stats["dissipation"]
     assert abs(o.total_energy(W) - float(g["ke"])) <= 1e-13 * float(g["ke"])
+
+
+def test_mdcd_hybrid_switch_is_discontinuous(oracle_mod):
+    """mdcd_hybrid_reconstruction (reconstruction.cpp:151-225) switches between
+    its linear and nonlinear stencils at min(sai1, sai2) = 0.4, so the
+    reference's own FP64 RHS jumps when a perturbation carries a face across
+    the threshold: on the 16^3 Taylor-Green box at Ma 0.1 a 1e-7 relative
+    perturbation of every variable moves the MDCD_HYBRID RHS by more than 1e-2
+    (max norm), against under 1e-3 for WENO5, while a 1e-9 perturbation of the
+    velocities moves both alike. This is why the FP32-stencil form, whose
+    split-flux deviations are rounded to float, is held to the FP32 bounds for
+    every scheme but this one."""
+    from ns3d_cpp_b200 import initial
+    n = 16
+    W = initial.taylor_green(n, Ma=0.1, perturb=0.05, seed=9)
+    moved = {}
+    for name, kw in (("hybrid", dict(vis_scheme="C6th", recon="MDCD_HYBRID")), ("weno5", {})):
+        o = oracle_mod.Oracle(ref_cfg(n, **kw))
+        r = o.rhs(W)
+        rng = np.random.default_rng(0)
+        Wa = W * (1 + 1e-7 * rng.standard_normal(W.shape))
+        Wv = W.copy()
+        Wv[1:4] *= 1 + 1e-9 * rng.standard_normal(Wv[1:4].shape)
+        moved[name] = (relerr(o.rhs(Wa), r).max(), relerr(o.rhs(Wv), r).max())
+    assert moved["hybrid"][0] > 1e-2 and moved["weno5"][0] < 1e-3, moved
+    assert moved["hybrid"][1] < 1e-6 and moved["weno5"][1] < 1e-6, moved
