@@ -738,7 +738,7 @@ namespace ns3d {
 void default_tiling(LaunchCfg& L) {
     L.zb = 0;
     L.tiled = 3;  // 2.5-D viscous flux, pipelined plane loads (k_visc_flux_pipe)
-    L.pipe = 1;   // FP32 x sweep with the software-pipelined split (k_sweep_x_pipe)
+    L.pipe = 3;   // FP32 sweeps with the software-pipelined split (k_sweep_x_pipe, k_sweep_pipe)
     if (const char* e = std::getenv("NS3D_PIPE")) L.pipe = std::atoi(e);
     if (const char* e = std::getenv("NS3D_TILE_ZB")) L.zb = std::atoi(e);
     if (const char* e = std::getenv("NS3D_TILED")) L.tiled = std::atoi(e);

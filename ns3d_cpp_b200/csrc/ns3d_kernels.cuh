@@ -1634,6 +1634,141 @@ k_sweep_ring(DevParams P, StateView W, R* __restrict__ tacc, int seg, const Ctrl
     }
 }
 
+// FP32-form y / z sweep with the split software-pipelined (k_sweep_ring's
+// march and arithmetic, reordered): when face f is reconstructed its whole
+// window (cells f-MID .. f-MID+S-1) is already in the ring, and the split of
+// cell f-MID+S, which enters the window of face f+1, runs in the same
+// iteration, beside the reconstruction and with no branch between the two
+// chains (ENT fixes the entropy-fix choice, square roots from sqrt_nr_nb); its
+// split flux goes into the slot of cell f-MID once the window has been read.
+// The interleaved chains need more registers than the 126 of the plain ring
+// at 4 blocks per SM, so this kernel is compiled for NS3D_PIPE_MINB blocks.
+#ifndef NS3D_PIPE_MINB
+#define NS3D_PIPE_MINB 3
+#endif
+template <int DIR, int FVS, int RC, int ENT>
+__global__ void __launch_bounds__(RingCfg<float>::T, NS3D_PIPE_MINB)
+k_sweep_pipe(DevParams P, StateView W, float* __restrict__ tacc, int seg,
+             const Ctrl* __restrict__ ctrl) {
+    static_assert(DIR == 1 || DIR == 2, "y and z sweeps");
+    constexpr int S = Stencil<RC>::S;
+    constexpr int MID = (S - 1) / 2;
+    constexpr int T = RingCfg<float>::T;
+    __shared__ SplitRing<float, S, T> ring;
+    if (ctrl && ctrl->stop) return;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = P.n;
+    const int tid = threadIdx.x;
+    const int t0 = blockIdx.x * blockDim.x + tid;
+    if (t0 >= nx) return;  // each thread owns its ring column: no barrier follows
+    const int len = DIR == 1 ? ny : nz;
+    const long long stride = DIR == 1 ? (long long)nx : (long long)nx * ny;
+    const long long base = DIR == 1 ? (long long)blockIdx.y * ny * nx + t0
+                                    : (long long)blockIdx.y * nx + t0;
+    const int c0 = blockIdx.z * seg;
+    if (c0 >= len) return;
+    const int c1 = min(c0 + seg, len);
+
+    float lin[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) lin[m] = float(P.lin[m]);
+    const float disp = float(P.mdcd_disp), diss = float(P.mdcd_diss);
+    const float inv_h = float(DIR == 1 ? P.inv_dy : P.inv_dz);
+    const double inv_gm1 = 1.0 / (P.gamma - 1.0);
+    const double inv_2g = 1.0 / (2.0 * P.gamma);
+    double refp[5], refm[5];
+    // cells f-MID .. f-MID+S+1 of every face: within (-len, 2 len) for
+    // extents >= 8, so one wrap suffices
+    auto load_raw = [&](int s, double* raw) {
+        const long long id = base + (long long)wrap1(s, len) * stride;
+        raw[0] = W.rho[id];
+        raw[1] = W.u[id];
+        raw[2] = W.v[id];
+        raw[3] = W.w[id];
+        raw[4] = W.p[id];
+    };
+    auto split_d = [&](const double* raw, double* Fpd, double* Fmd) {
+        split_fast<FVS, 0, DIR == 1, DIR == 2, 1, ENT, true>(P, inv_gm1, inv_2g, raw, Fpd, Fmd);
+    };
+    auto split_raw = [&](const double* raw, float* Fp, float* Fm) {
+        double Fpd[5], Fmd[5];
+        split_d(raw, Fpd, Fmd);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            Fp[q] = float(Fpd[q] - refp[q]);
+            Fm[q] = float(Fmd[q] - refm[q]);
+        }
+    };
+
+    int f = c0 - 1;  // face f sits between cells f and f+1
+    double nxt[5];
+    {
+        // the window of face c0-1 into slots 0..S-1; its first cell's split
+        // flux is the segment's offset
+        float Fp[5], Fm[5];
+        load_raw(f - MID, nxt);
+        split_d(nxt, refp, refm);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) Fp[q] = Fm[q] = 0.f;
+        ring.put(0, tid, Fp, Fm);
+#pragma unroll
+        for (int m = 1; m < S; ++m) {
+            load_raw(f - MID + m, nxt);
+            split_raw(nxt, Fp, Fm);
+            ring.put(m, tid, Fp, Fm);
+        }
+    }
+    load_raw(f - MID + S, nxt);
+    float prev[5];
+    int ph = 0;  // window position m of the current face sits in slot (ph + m) mod S
+    for (int t = 0; f < c1; ++t, ++f) {
+        double cur[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) cur[q] = nxt[q];
+        load_raw(f - MID + S + 1, nxt);  // split in the next iteration
+        const long long oid = base + (long long)f * stride;
+        float old[5];
+        if (t > 0) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) old[q] = tacc[q * n + oid];
+        }
+        float face[5], Fp[5], Fm[5];
+        if constexpr (RC == RC_WENO5) {
+            float fp[S][5], fm[S][5];
+            ring_window_at(ph, ring, tid, fp, fm);
+            split_raw(cur, Fp, Fm);
+            weno5_face_x2([&](int m, int q) { return fp[m][q]; },
+                          [&](int m, int q) { return fm[S - 1 - m][q]; }, face);
+        } else {
+            int sl[S];
+#pragma unroll
+            for (int m = 0; m < S; ++m) sl[m] = ph + m < S ? ph + m : ph + m - S;
+            split_raw(cur, Fp, Fm);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                float a[S], b[S];
+#pragma unroll
+                for (int m = 0; m < S; ++m) {
+                    a[m] = ring.comp(sl[m], tid, q, false);
+                    b[m] = ring.comp(sl[S - 1 - m], tid, q, true);
+                }
+                const float plus_face = reconstruct<float, RC>(a, lin, disp, diss);
+                const float minus_face = reconstruct<float, RC>(b, lin, disp, diss);
+                face[q] = plus_face + minus_face;
+            }
+        }
+        // cell f-MID leaves the window: its slot takes cell f-MID+S
+        ring.put(ph, tid, Fp, Fm);
+        if (t > 0) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) tacc[q * n + oid] = old[q] + (face[q] - prev[q]) * inv_h;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) prev[q] = face[q];
+        ph = ph + 1 == S ? 0 : ph + 1;
+    }
+}
+
 // Sums of the reductions below (see k_sums_partial).
 constexpr int NSUMS = 13;
 

@@ -20,8 +20,8 @@ struct LaunchCfg {
     cudaStream_t stream;
     int zb;       // planes per block of the 2.5-D viscous kernels (0: from the grid)
     int tiled;    // bit 0: 2.5-D visc_flux (when the box tiles); bit 1: its pipelined form
-    int pipe;     // 1: the FP32 x sweep with the software-pipelined split (k_sweep_x_pipe,
-                  // rows of >= 128 cells); 0: k_sweep_x_warp_f32
+    int pipe;     // FP32 sweeps with the software-pipelined split: bit 0 the x sweep
+                  // (k_sweep_x_pipe, rows of >= 128 cells), bit 1 the y / z sweeps (k_sweep_pipe)
 };
 
 // Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED / NS3D_SEG for tuning.
@@ -93,7 +93,7 @@ cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl
         const long long rows = (long long)P.ny * P.nz;
         const unsigned blocks = (unsigned)((rows + XW_WARPS - 1) / XW_WARPS);
         if constexpr (sizeof(R) == 4 && !CHR) {
-            if (L.pipe && P.nx >= 128) {
+            if ((L.pipe & 1) && P.nx >= 128) {
                 if constexpr (FVS == FV_SW) {
                     if (P.sw_eps > 0.0) {  // the entropy fix, compiled in
                         k_sweep_x_pipe<FVS, RC, 1><<<blocks, 32 * XW_WARPS, 0, L.stream>>>(P, W, tacc, ctrl);
@@ -111,6 +111,18 @@ cudaError_t sweep_dir(const LaunchCfg& L, StateView W, R* tacc, const Ctrl* ctrl
     }
     if constexpr (DIR != 0 && !CHR) {
         const MarchShape m = march_shape<DIR>(L, RingCfg<R>::T);
+        if constexpr (sizeof(R) == 4) {
+            if (L.pipe & 2) {
+                if constexpr (FVS == FV_SW) {
+                    if (P.sw_eps > 0.0) {  // the entropy fix, compiled in
+                        k_sweep_pipe<DIR, FVS, RC, 1><<<m.grid, m.th, 0, L.stream>>>(P, W, tacc, m.seg, ctrl);
+                        return cudaGetLastError();
+                    }
+                }
+                k_sweep_pipe<DIR, FVS, RC, 0><<<m.grid, m.th, 0, L.stream>>>(P, W, tacc, m.seg, ctrl);
+                return cudaGetLastError();
+            }
+        }
         k_sweep_ring<DIR, R, FVS, RC, false><<<m.grid, m.th, 0, L.stream>>>(
             P, W, tacc, m.seg, ctrl, FuseArgs<R>{});
         return cudaGetLastError();

@@ -7,13 +7,13 @@ is created). Both perform the same floating-point operations per cell in the
 same order, so the states, the CFL dt and the time loop's step counts must
 agree exactly.
 
-The FP32 form's x sweep with the split software-pipelined beside the
-reconstruction (k_sweep_x_pipe; NS3D_PIPE=0 selects k_sweep_x_warp_f32)
-evaluates the same formulas, but the compiler contracts its double split into
-FMAs in its own way, so the two agree to float rounding of the split-flux
-deviations rather than bit for bit; both sit within the FP32 form's bounds
-against the FP64 oracle (the 256^3 RHS in test_size_parity takes the
-pipelined sweep).
+The FP32 form's sweeps with the split software-pipelined beside the
+reconstruction (k_sweep_x_pipe, k_sweep_pipe; NS3D_PIPE=0 selects
+k_sweep_x_warp_f32 and k_sweep_ring) evaluate the same formulas, but the
+compiler contracts their double split into FMAs in its own way, so the two
+agree to float rounding of the split-flux deviations rather than bit for bit;
+both sit within the FP32 form's bounds against the FP64 oracle (the 256^3 RHS
+in test_size_parity takes the pipelined sweeps).
 """
 import os
 
@@ -28,7 +28,7 @@ from test_gpu_parity import params_from_cfg
 pytestmark = pytest.mark.gpu
 
 SCHEDULES = {"plain": {}, "fuse_z": {"NS3D_FUSE": "1"}}
-PIPE_SCHEDULES = {"plain": {"NS3D_PIPE": "0"}, "pipelined": {"NS3D_PIPE": "1"}}
+PIPE_SCHEDULES = {"plain": {"NS3D_PIPE": "0"}, "pipelined": {"NS3D_PIPE": "3"}}
 
 
 def _solver(params, env):
@@ -95,9 +95,9 @@ def test_fused_time_loop_stops_identically():
 
 
 @pytest.mark.parametrize("kw", SCHEMES + [dict(sw_entropy_eps=1e-3)], ids=scheme_id)
-def test_pipelined_x_sweep_matches_plain(kw, oracle_mod):
+def test_pipelined_sweeps_match_plain(kw, oracle_mod):
     """FP32 form, 128 x 32 x 40 Taylor-Green box at Ma 0.3 (rows of four 32-cell
-    chunks, the pipelined sweep's smallest case): the RHS with and without the
+    chunks, the pipelined x sweep's smallest case): the RHS with and without the
     pipelined split within 1e-6 (the rounding of one float split-flux deviation
     moves a face flux by ~1e-7 of the RHS scale), as close to the FP64 oracle
     as the plain sweep's (and within the FP32 form's 5e-5 for SW + WENO5), and
