@@ -24,7 +24,8 @@ struct LaunchCfg {
                   // (k_sweep_x_pipe, rows of >= 128 cells), bit 1 the y / z sweeps (k_sweep_pipe)
 };
 
-// Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED / NS3D_SEG for tuning.
+// Launch-shape defaults, overridable by NS3D_TILE_ZB / NS3D_TILED / NS3D_SEG / NS3D_PIPE for
+// tuning.
 void default_tiling(LaunchCfg& L);
 
 // One inviscid sweep (dir 0, 1, 2 in this order per RHS evaluation).
